@@ -1,0 +1,185 @@
+/*
+ * doubleeye_b200 -- C ABI of the B200 (sm_100a) stereo hot path:
+ * Census -> graded Census/AD cost -> 4-pass recursive edge-aware filter ->
+ * per-pixel top-2 -> MASDA row solve (dense), and keypoint MASDA (sparse).
+ *
+ * Conventions (every entry point):
+ *   - returns an int status: DE_OK (0) or a negative DE_ERR_*; never exits;
+ *     de_last_error() gives a one-line reason for the calling thread.
+ *   - buffers are caller-owned.  Functions named *_dev take DEVICE pointers and
+ *     enqueue on the given cudaStream_t (passed as void*, NULL = legacy default
+ *     stream) without allocating; their scratch is a caller-provided workspace
+ *     sized by the matching *_workspace_bytes() call.  Functions on a de_ctx take
+ *     HOST pointers, copy through pinned staging, and block until done.
+ *   - a de_ctx is safe to use from one thread at a time; distinct contexts are
+ *     independent (one CUDA stream each).
+ *   - only plain C types cross the boundary; no torch or CUDA types appear here.
+ *
+ * Reference interfaces replaced (paths within mayio/doubleeye):
+ *   core/include/doubleeye/dense_solve.hpp:19-97     Cfg            -> de_cfg
+ *   core/tools/de_dense.cpp:94-129,186-227           census_image   -> de_census_dev
+ *   core/tools/de_dense.cpp:531-561                  rf_coeffs      -> de_census_dev (ax/ay)
+ *   core/tools/de_dense.cpp:1198-1297                score/filter/top-2 -> de_cost_top2_dev
+ *   core/tools/de_dense_cuda.cu:159-392              k_score_hfwd..k_vert_bwd_top2 -> de_cost_top2_dev
+ *   core/include/doubleeye/dense_solve.hpp:213-452   solve_row_sparse -> de_solve_dev
+ *   core/tools/de_dense.cpp:738-1608                 run_dense      -> de_dense_dev / de_ctx_dense
+ *   core/include/doubleeye/dense_solve.hpp:158-171   confidence(_u8) -> de_confidence
+ *   core/include/doubleeye/preproc.hpp:96-97         census_at      -> de_census_at_dev
+ *   core/include/doubleeye/preproc.hpp:202-204       detect_keypoints_fast -> de_detect_fast_dev
+ *   core/include/doubleeye/match.hpp:221-226         match_masda    -> de_match_masda_dev
+ *   article/masda_stereo.py:453-492                  masda_sparse   -> de_masda_edges_dev
+ */
+#ifndef DOUBLEEYE_B200_H
+#define DOUBLEEYE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DE_API __attribute__((visibility("default")))
+
+enum {
+  DE_OK = 0,
+  DE_ERR_ARG = -1,         /* bad argument or size beyond a documented limit */
+  DE_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  DE_ERR_OOM = -3,         /* device or pinned allocation failed */
+  DE_ERR_TIMEOUT = -4,     /* a bounded device wait ran out */
+  DE_ERR_UNSUPPORTED = -5, /* configuration outside this build's arithmetic */
+  DE_ERR_BUSY = -6,        /* admission refused: HBM budget or queue full */
+  DE_ERR_CLOSED = -7       /* the server was stopped */
+};
+
+/* Dense matcher configuration.  Field meaning and defaults follow
+ * core/include/doubleeye/dense_solve.hpp:19-97 (Cfg) for the fields this path
+ * reads; de_cfg_default() writes those defaults. */
+typedef struct de_cfg {
+  int dmin, dmax;          /* disparities searched, dmin..dmax (default 1..60) */
+  int iters;               /* MASDA message-passing iterations (default 0 = WTA) */
+  float sigma_s, sigma_r;  /* recursive-filter reach and edge sensitivity (8, 0.2) */
+  float ad;                /* weight of the truncated absolute difference (0.15) */
+  int ad_trunc;            /* AD saturation, 8-bit levels (10) */
+  float lambda, gamma;     /* clutter / misdetection costs (-0.1, -0.1) */
+  float damping;           /* message damping (0.4) */
+  float min_margin;        /* best-minus-second gate, 0 = off */
+  float min_ratio;         /* peak-ratio gate, 0 = off */
+  int subpixel;            /* sub-pixel fit on (1) */
+  int fit_eq;              /* equiangular fit (1) or parabola (0) */
+  int lrc;                 /* exact reverse match over every disparity (0) */
+  int census_hw, census_hh;/* census half-window; 3,3 (7x7) is the reference's */
+} de_cfg;
+
+DE_API void de_cfg_default(de_cfg* cfg);
+
+/* Limits of this build: D = dmax - dmin + 1 <= 256 (8-bit k in the packed top-2
+ * key), 8 <= W <= 8192, 8 <= H <= 8192, dmin >= 1. */
+#define DE_MAX_D 256
+#define DE_MAX_DIM 8192
+
+DE_API const char* de_last_error(void);
+DE_API const char* de_version(void);
+
+/* ---- dense, device pointers, caller workspace, asynchronous ------------------ */
+
+/* One stereo pair.  L/R are W*H u8 rows of pitch W (device).  Outputs (device,
+ * W*H each, any may be NULL): disp f32 (NaN = declined), margin f32, conf u8
+ * (confidence_u8, 0 where declined), cand f32 planes in the reference's
+ * --out-conf order s1,s2,d1,d2,lrc,lrc2 (6*W*H).  dmax 0 = the cfg's. */
+typedef struct de_pair {
+  const uint8_t* L;
+  const uint8_t* R;
+  int W, H, dmax;
+  float* disp;
+  float* margin;
+  uint8_t* conf;
+  float* cand;
+} de_pair;
+
+/* Workspace for de_dense_dev on n pairs (sum over pairs, 256-byte aligned). */
+DE_API int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int n,
+                                    size_t* bytes);
+/* Census -> cost -> filter -> top-2 -> row solve for n pairs in one set of
+ * launches (pairs may differ in W, H and dmax).  Replaces run_dense
+ * (core/tools/de_dense.cpp:738) and the de_dense_cuda pipeline
+ * (core/tools/de_dense_cuda.cu:556-663). */
+DE_API int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n,
+                        void* workspace, size_t ws_bytes, void* stream);
+
+/* Stage entry points, for stage-level parity and for callers that keep their
+ * own pipeline.  Census planes: cl/cr u64 (0 on the border), ax/ay u16 Q15
+ * filter coefficients of the LEFT image (core/tools/de_dense.cpp:531-561). */
+DE_API int de_census_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W,
+                         int H, uint64_t* cl, uint64_t* cr, uint16_t* ax, uint16_t* ay,
+                         void* stream);
+/* Candidates in the reference layout (core/tools/de_dense_cuda.cu:286-392):
+ * cs f32[2WH] (Q14/16384), cd i32[2WH] (k = d - dmin), cn i32[WH],
+ * cnb i16[2WH] (filtered cost at k*-1, k*+1 in Q14; -32768 = none, may be NULL).
+ * cs/cd slots j >= cn are unspecified. */
+DE_API size_t de_cost_workspace_bytes(int W, int H, int D);
+DE_API int de_cost_top2_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R,
+                            int W, int H, float* cs, int* cd, int* cn, int16_t* cnb,
+                            void* workspace, size_t ws_bytes, void* stream);
+/* Row solve over reference-layout candidates (dense_solve.hpp:213-452 with K=2,
+ * vol = NULL): disp, margin, lrc2 f32[WH] (lrc2 may be NULL). */
+DE_API int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const int* cd,
+                        const int* cn, const int16_t* cnb, float* disp, float* margin,
+                        float* lrc2, void* stream);
+
+/* confidence() / confidence_u8() of dense_solve.hpp:158-171, host side. */
+DE_API float de_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol);
+
+/* ---- sparse (keypoint) MASDA ------------------------------------------------- */
+
+/* Keypoint of core/include/doubleeye/preproc.hpp:125-130. */
+typedef struct de_keypoint { float x, y, response, local_std; } de_keypoint;
+
+/* DetectorConfig of core/include/doubleeye/preproc.hpp:132-145, same defaults. */
+typedef struct de_det_cfg {
+  int grad_window, cell, per_cell;
+  float min_response, min_local_std;
+  int border, subpixel, fast_threshold, nms_radius;
+} de_det_cfg;
+DE_API void de_det_cfg_default(de_det_cfg* cfg);
+
+/* MatchConfig of core/include/doubleeye/match.hpp:135-176 (priors excluded), same
+ * defaults.  census_bits is the descriptor length the score is scaled by; the
+ * reference hard-codes 48 (core/src/match.cpp:339) and so does the default. */
+typedef struct de_match_cfg {
+  float max_dy, min_disparity, max_disparity;
+  int max_candidates;
+  float sigma_y, w_y;
+  int iterations;
+  float damping, lambda, gamma, converge_eps;
+  int census_bits;
+} de_match_cfg;
+DE_API void de_match_cfg_default(de_match_cfg* cfg);
+
+/* Match / MatchStats of core/include/doubleeye/match.hpp:44-66,178-186. */
+typedef struct de_match {
+  int left, right;
+  float score, belief, disparity, dy, margin;
+} de_match;
+typedef struct de_match_stats {
+  int left, right, candidates, iterations_run, converged;
+  float final_max_delta;
+  int oscillating;
+} de_match_stats;
+
+/* ---- dense, host pointers, context-owned memory, synchronous ----------------- */
+
+typedef struct de_ctx de_ctx;
+DE_API int de_ctx_create(const de_cfg* cfg, int device, de_ctx** out);
+DE_API int de_ctx_destroy(de_ctx* ctx);
+DE_API int de_ctx_set_cfg(de_ctx* ctx, const de_cfg* cfg);
+/* Host-buffer single pair: uploads L/R, runs de_dense_dev, downloads outputs. */
+DE_API int de_ctx_dense(de_ctx* ctx, const uint8_t* L, const uint8_t* R, int W, int H,
+                        float* disp, float* margin, uint8_t* conf, float* cand);
+/* The same for n host pairs in one batched launch. */
+DE_API int de_ctx_dense_batch(de_ctx* ctx, const de_pair* host_pairs, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DOUBLEEYE_B200_H */

@@ -1,0 +1,56 @@
+/*
+ * ORACLE -- test infrastructure, not product code.
+ *
+ * A plain-C, single-threaded restatement of the reference algorithm for the
+ * stereo hot path (mayio/doubleeye core/tools/de_dense.cpp,
+ * core/include/doubleeye/dense_solve.hpp, core/src/preproc.cpp,
+ * core/src/match.cpp).  Only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg load it, and only as the checker.  Each function cites the
+ * reference lines it restates.
+ *
+ * Pinned: tests/test_oracle_golden.py checks every function below against
+ * golden vectors produced by the reference itself (oracle/_ref, built from the
+ * reference sources by oracle/Makefile; fixtures made by
+ * tests/golden/make_golden.py).
+ *
+ * Deliberate difference: where the reference orders by std::sort (unstable;
+ * libstdc++'s tie order is implementation-defined), this oracle uses a total
+ * order with an index tie-break.  Results agree except between exactly tied
+ * claimants.
+ */
+#ifndef DE_ORACLE_H
+#define DE_ORACLE_H
+
+#include <stdint.h>
+#include "doubleeye_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+void or_census(const uint8_t* img, int W, int H, int hw, int hh, uint64_t* out);
+void or_rf_lut(float sigma_s, float sigma_r, uint16_t lut[256]);
+void or_rf_coeffs(const uint8_t* L, int W, int H, const uint16_t lut[256], uint16_t* ax,
+                  uint16_t* ay);
+int or_score_tables(const de_cfg* cfg, int16_t tbl[65], int16_t adt[256]);
+void or_filter_i16(int16_t* plane, const uint16_t* ax, const uint16_t* ay, int W, int H);
+void or_filter_f64(double* plane, const uint16_t* ax, const uint16_t* ay, int W, int H);
+void or_score_plane(const de_cfg* cfg, const uint8_t* L, const uint8_t* R,
+                    const uint64_t* cl, const uint64_t* cr, int W, int H, int k,
+                    int16_t* plane);
+void or_cost_top2(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                  float* cs, int* cd, int* cn, int16_t* cnb, int16_t* rbest_k);
+void or_solve_row(const de_cfg* cfg, int W, const float* cs, const int* cd, const int* cn,
+                  const int16_t* cnb, float* disp, float* margin, float* lrc2);
+void or_solve_row_debug(const de_cfg* cfg, int W, const float* cs, const int* cd,
+                        const int* cn, const int16_t* cnb, float* disp, float* margin,
+                        float* lrc2, float* best_out, int* target_out);
+void or_dense(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+              float* disp, float* margin, float* cand6);
+float or_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol);
+unsigned or_confidence_u8(float s1, float s2, float lambda, float lrc, float lrc_tol);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

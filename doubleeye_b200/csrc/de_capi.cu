@@ -1,0 +1,541 @@
+// C ABI of the B200 stereo hot path: argument checking, workspace planning, the
+// host-built arithmetic tables, the batch descriptor table, and the host-pointer
+// context.  See include/doubleeye_b200.h for the contract of every entry point.
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "de_internal.h"
+
+namespace {
+
+thread_local char g_err[512] = "";
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  const int code = (e == cudaErrorMemoryAllocation) ? DE_ERR_OOM : DE_ERR_CUDA;
+  return fail(code, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define DE_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v) { return (v + kAlign - 1) & ~(kAlign - 1); }
+
+int census_bits(const de_cfg& c) {
+  return (2 * c.census_hw + 1) * (2 * c.census_hh + 1) - 1;
+}
+
+int check_cfg(const de_cfg* c) {
+  if (!c) return fail(DE_ERR_ARG, "cfg is NULL");
+  if (c->dmin < 1) return fail(DE_ERR_ARG, "dmin must be >= 1 (got %d)", c->dmin);
+  const int D = c->dmax - c->dmin + 1;
+  if (D < 1 || D > DE_MAX_D)
+    return fail(DE_ERR_ARG, "disparity count dmax-dmin+1 = %d outside 1..%d", D, DE_MAX_D);
+  if (c->census_hw < 1 || c->census_hh < 1 || c->census_hw > 4 || c->census_hh > 4 ||
+      census_bits(*c) > 64)
+    return fail(DE_ERR_ARG, "census half-window %dx%d unsupported (<= 4, <= 64 bits)",
+                c->census_hw, c->census_hh);
+  if (!(c->sigma_s > 0.f) || !(c->sigma_r > 0.f))
+    return fail(DE_ERR_ARG, "sigma_s and sigma_r must be positive");
+  if (c->iters < 0) return fail(DE_ERR_ARG, "iters must be >= 0");
+  return DE_OK;
+}
+
+int check_dims(int W, int H) {
+  if (W < 8 || H < 8 || W > de::kMaxW || H > de::kMaxH)
+    return fail(DE_ERR_ARG, "image %dx%d outside 8..%d x 8..%d", W, H, de::kMaxW, de::kMaxH);
+  return DE_OK;
+}
+
+}  // namespace
+
+namespace de {
+
+// Host-built tables, the same expressions as the reference so the values agree bit
+// for bit: the filter LUT core/tools/de_dense.cpp:533-546 (float, std::exp), the
+// score tables :1201-1223.
+void make_dev_cfg(const de_cfg& c, DevCfg* o) {
+  std::memset(o, 0, sizeof(*o));
+  o->dmin = c.dmin;
+  o->iters = c.iters;
+  o->hw = c.census_hw;
+  o->hh = c.census_hh;
+  o->subpixel = c.subpixel != 0;
+  o->fit_eq = c.fit_eq != 0;
+  o->lrc = c.lrc != 0;
+  o->lambda = c.lambda;
+  o->gamma = c.gamma;
+  o->damping = c.damping;
+  o->keep = 1.f - c.damping;
+  o->min_margin = c.min_margin;
+  o->min_ratio = c.min_ratio;
+  const int nbits = census_bits(c);
+  o->packed = nbits <= 56;
+  const int half = nbits / 2;
+  for (int h = 0; h <= 2 * half && h < 66; ++h)
+    o->tbl[h] = int16_t(((half - h) * 16384) / half);
+  const float adc = std::max(0.f, std::min(1.f, c.ad));
+  o->wq = int32_t(adc * 1024.f);
+  const int T = std::max(1, c.ad_trunc);
+  o->trunc = T;
+  for (int v = 0; v < 256; ++v)
+    o->adt[v] = int16_t(16384 - (2 * 16384 * std::min(v, T)) / T);
+  const float kk = -std::sqrt(2.f) / c.sigma_s;
+  const float rs = c.sigma_s / c.sigma_r;
+  for (int d = 0; d < 256; ++d) {
+    const float e = std::exp(kk * (1.f + rs * (float(d) / 255.f)));
+    o->rf[d] = uint16_t(std::min(32767.f, e * 32768.f + 0.5f));
+  }
+}
+
+static int dpad_of(int D) { return (D + 63) & ~63; }
+
+size_t pair_workspace_bytes(int W, int H, int D, bool lrc) {
+  const size_t WH = size_t(W) * H;
+  size_t s = 0;
+  s += align_up(WH * 8) * 2;                      // census words L, R
+  s += align_up(WH * 2) * 2;                      // ax, ay
+  s += align_up(WH * size_t(dpad_of(D)) * 2);     // filtered volume
+  s += align_up(WH * 4) * 3;                      // key0, key1, nb
+  if (lrc) s += align_up(WH * 4);                 // reverse-match keys
+  return s;
+}
+
+void carve_pair(DevPair* p, void* ws, int W, int H, int D, bool lrc) {
+  const size_t WH = size_t(W) * H;
+  uint8_t* c = static_cast<uint8_t*>(ws);
+  auto take = [&](size_t bytes) { uint8_t* r = c; c += align_up(bytes); return r; };
+  p->cwL = reinterpret_cast<uint64_t*>(take(WH * 8));
+  p->cwR = reinterpret_cast<uint64_t*>(take(WH * 8));
+  p->ax = reinterpret_cast<uint16_t*>(take(WH * 2));
+  p->ay = reinterpret_cast<uint16_t*>(take(WH * 2));
+  p->vol = reinterpret_cast<int16_t*>(take(WH * size_t(dpad_of(D)) * 2));
+  p->key0 = reinterpret_cast<uint32_t*>(take(WH * 4));
+  p->key1 = reinterpret_cast<uint32_t*>(take(WH * 4));
+  p->nb = reinterpret_cast<uint32_t*>(take(WH * 4));
+  p->rkey = lrc ? reinterpret_cast<uint32_t*>(take(WH * 4)) : nullptr;
+  p->W = W;
+  p->H = H;
+  p->D = D;
+  p->Dpad = dpad_of(D);
+}
+
+}  // namespace de
+
+namespace {
+
+int pair_D(const de_cfg& c, const de_pair& p) {
+  const int dmax = p.dmax > 0 ? p.dmax : c.dmax;
+  return dmax - c.dmin + 1;
+}
+
+int check_pair(const de_cfg& c, const de_pair& p) {
+  int rc = check_dims(p.W, p.H);
+  if (rc) return rc;
+  const int D = pair_D(c, p);
+  if (D < 1 || D > DE_MAX_D)
+    return fail(DE_ERR_ARG, "pair disparity count %d outside 1..%d", D, DE_MAX_D);
+  if (!p.L || !p.R) return fail(DE_ERR_ARG, "pair images are NULL");
+  return DE_OK;
+}
+
+// Fill one launch set's descriptor table for pairs[first, first+n).
+void fill_batch(const de_cfg& c, const de_pair* pairs, int first, int n, uint8_t* ws,
+                de::Batch* b) {
+  std::memset(b, 0, sizeof(*b));
+  b->n = n;
+  const int hh = c.census_hh, hw = c.census_hw;
+  for (int i = 0; i < n; ++i) {
+    const de_pair& p = pairs[first + i];
+    const int D = pair_D(c, p);
+    de::DevPair& d = b->p[i];
+    de::carve_pair(&d, ws, p.W, p.H, D, c.lrc != 0);
+    ws += de::pair_workspace_bytes(p.W, p.H, D, c.lrc != 0);
+    d.L = p.L;
+    d.R = p.R;
+    d.disp = p.disp;
+    d.margin = p.margin;
+    d.conf = p.conf;
+    d.cand = p.cand;
+    b->maxDpad = std::max(b->maxDpad, d.Dpad);
+    const int tiles = ((p.W + 31) / 32) * ((p.H + 7) / 8);
+    b->pix_prefix[i + 1] = b->pix_prefix[i] + tiles;
+    b->rows_prefix[i + 1] = b->rows_prefix[i] + std::max(0, p.H - 2 * hh);
+    b->cols_prefix[i + 1] = b->cols_prefix[i] + std::max(0, p.W - 2 * hw - c.dmin);
+    b->solve_prefix[i + 1] = b->solve_prefix[i] + p.H;
+  }
+}
+
+int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
+  de::DevCfg dc;
+  de::make_dev_cfg(c, &dc);
+  if (c.lrc)
+    for (int i = 0; i < b.n; ++i)
+      DE_CUDA(cudaMemsetAsync(b.p[i].rkey, 0, size_t(b.p[i].W) * b.p[i].H * 4, s));
+  DE_CUDA(de::launch_census(dc, b, s));
+  DE_CUDA(de::launch_rows(dc, b, s));
+  DE_CUDA(de::launch_cols(dc, b, s));
+  DE_CUDA(de::launch_solve(dc, b, false, s));
+  return DE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* de_last_error(void) { return g_err; }
+const char* de_version(void) { return "doubleeye_b200 0.1 (sm_100a)"; }
+
+void de_cfg_default(de_cfg* c) {
+  if (!c) return;
+  c->dmin = 1;
+  c->dmax = 60;
+  c->iters = 0;
+  c->sigma_s = 8.f;
+  c->sigma_r = 0.20f;
+  c->ad = 0.15f;
+  c->ad_trunc = 10;
+  c->lambda = -0.1f;
+  c->gamma = -0.1f;
+  c->damping = 0.4f;
+  c->min_margin = 0.f;
+  c->min_ratio = 0.f;
+  c->subpixel = 1;
+  c->fit_eq = 1;
+  c->lrc = 0;
+  c->census_hw = 3;
+  c->census_hh = 3;
+}
+
+void de_det_cfg_default(de_det_cfg* c) {
+  if (!c) return;
+  c->grad_window = 3;
+  c->cell = 32;
+  c->per_cell = 3;
+  c->min_response = 1.0f;
+  c->min_local_std = 2.0f;
+  c->border = 8;
+  c->subpixel = 1;
+  c->fast_threshold = 8;
+  c->nms_radius = 3;
+}
+
+void de_match_cfg_default(de_match_cfg* c) {
+  if (!c) return;
+  c->max_dy = 2.0f;
+  c->min_disparity = 1.0f;
+  c->max_disparity = 220.0f;
+  c->max_candidates = 24;
+  c->sigma_y = 1.0f;
+  c->w_y = 1.0f;
+  c->iterations = 20;
+  c->damping = 0.4f;
+  c->lambda = 0.0f;
+  c->gamma = 0.0f;
+  c->converge_eps = 1e-4f;
+  c->census_bits = 48;
+}
+
+int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int n,
+                             size_t* bytes) {
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  if (!bytes || n < 0 || (n > 0 && !pairs)) return fail(DE_ERR_ARG, "bad arguments");
+  size_t s = 0;
+  for (int i = 0; i < n; ++i) {
+    if ((rc = check_pair(*cfg, pairs[i]))) return rc;
+    s += de::pair_workspace_bytes(pairs[i].W, pairs[i].H, pair_D(*cfg, pairs[i]),
+                                  cfg->lrc != 0);
+  }
+  *bytes = s;
+  return DE_OK;
+}
+
+int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace,
+                 size_t ws_bytes, void* stream) {
+  size_t need = 0;
+  int rc = de_dense_workspace_bytes(cfg, pairs, n, &need);
+  if (rc) return rc;
+  if (need > ws_bytes || (need && !workspace))
+    return fail(DE_ERR_ARG, "workspace %zu bytes, need %zu", ws_bytes, need);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  static de::Batch b;          // large; filled and consumed under the lock
+  static std::mutex mu;
+  for (int first = 0; first < n; first += de::kMaxBatch) {
+    const int m = std::min(de::kMaxBatch, n - first);
+    std::lock_guard<std::mutex> lk(mu);
+    fill_batch(*cfg, pairs, first, m, ws, &b);
+    for (int i = 0; i < m; ++i)
+      ws += de::pair_workspace_bytes(pairs[first + i].W, pairs[first + i].H,
+                                     pair_D(*cfg, pairs[first + i]), cfg->lrc != 0);
+    if ((rc = run_batch(*cfg, b, s))) return rc;
+  }
+  return DE_OK;
+}
+
+int de_census_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                  uint64_t* cl, uint64_t* cr, uint16_t* ax, uint16_t* ay, void* stream) {
+  int rc = check_cfg(cfg);
+  if (rc || (rc = check_dims(W, H))) return rc;
+  if (!L || !R || !cl || !cr || !ax || !ay) return fail(DE_ERR_ARG, "NULL buffer");
+  de::DevCfg dc;
+  de::make_dev_cfg(*cfg, &dc);
+  dc.packed = 0;                               // plain census words for callers
+  static de::Batch b;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  std::memset(&b, 0, sizeof(b));
+  b.n = 1;
+  b.p[0].L = L; b.p[0].R = R; b.p[0].cwL = cl; b.p[0].cwR = cr; b.p[0].ax = ax;
+  b.p[0].ay = ay; b.p[0].W = W; b.p[0].H = H;
+  b.pix_prefix[1] = ((W + 31) / 32) * ((H + 7) / 8);
+  DE_CUDA(de::launch_census(dc, b, static_cast<cudaStream_t>(stream)));
+  return DE_OK;
+}
+
+size_t de_cost_workspace_bytes(int W, int H, int D) {
+  return de::pair_workspace_bytes(W, H, D, false);
+}
+
+int de_cost_top2_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                     float* cs, int* cd, int* cn, int16_t* cnb, void* workspace,
+                     size_t ws_bytes, void* stream) {
+  int rc = check_cfg(cfg);
+  if (rc || (rc = check_dims(W, H))) return rc;
+  if (!L || !R || !cs || !cd || !cn) return fail(DE_ERR_ARG, "NULL buffer");
+  const int D = cfg->dmax - cfg->dmin + 1;
+  const size_t need = de::pair_workspace_bytes(W, H, D, false);
+  if (ws_bytes < need || !workspace)
+    return fail(DE_ERR_ARG, "workspace %zu bytes, need %zu", ws_bytes, need);
+  de_cfg c2 = *cfg;
+  c2.lrc = 0;
+  de::DevCfg dc;
+  de::make_dev_cfg(c2, &dc);
+  static de::Batch b;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  de_pair p{};
+  p.L = L; p.R = R; p.W = W; p.H = H;
+  fill_batch(c2, &p, 0, 1, static_cast<uint8_t*>(workspace), &b);
+  b.p[0].ref_cs = cs; b.p[0].ref_cd = cd; b.p[0].ref_cn = cn; b.p[0].ref_cnb = cnb;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DE_CUDA(de::launch_census(dc, b, s));
+  DE_CUDA(de::launch_rows(dc, b, s));
+  DE_CUDA(de::launch_cols(dc, b, s));
+  DE_CUDA(de::launch_export_candidates(dc, b, s));
+  return DE_OK;
+}
+
+int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const int* cd,
+                 const int* cn, const int16_t* cnb, float* disp, float* margin,
+                 float* lrc2, void* stream) {
+  int rc = check_cfg(cfg);
+  if (rc || (rc = check_dims(W, H))) return rc;
+  if (!cs || !cd || !cn || !disp) return fail(DE_ERR_ARG, "NULL buffer");
+  de_cfg c2 = *cfg;
+  c2.lrc = 0;
+  de::DevCfg dc;
+  de::make_dev_cfg(c2, &dc);
+  static de::Batch b;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  std::memset(&b, 0, sizeof(b));
+  b.n = 1;
+  de::DevPair& P = b.p[0];
+  P.W = W; P.H = H;
+  P.ref_cs = const_cast<float*>(cs);
+  P.ref_cd = const_cast<int*>(cd);
+  P.ref_cn = const_cast<int*>(cn);
+  P.ref_cnb = const_cast<int16_t*>(cnb);
+  P.disp = disp; P.margin = margin; P.lrc2 = lrc2;
+  b.solve_prefix[1] = H;
+  DE_CUDA(de::launch_solve(dc, b, true, static_cast<cudaStream_t>(stream)));
+  return DE_OK;
+}
+
+// confidence(), core/include/doubleeye/dense_solve.hpp:158-166.
+float de_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol) {
+  if (!(s1 > -1e29f)) return 0.f;
+  const float alt = (s2 > -1e29f) ? std::max(s2, lambda) : lambda;
+  const float x = std::log(std::max((1.f - alt) / std::max(1.f - s1, 1e-6f), 1e-6f));
+  const float logit = 0.692684f + 7.936751f * x;
+  const float p = 1.f / (1.f + std::exp(-std::max(-30.f, std::min(30.f, logit))));
+  return (lrc > lrc_tol) ? std::min(p, 0.35f) : p;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// Host-pointer context: pinned staging, device buffers and workspace grown on
+// demand, one stream.
+struct de_ctx {
+  de_cfg cfg;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  void* dws = nullptr;        size_t dws_cap = 0;
+  void* dio = nullptr;        size_t dio_cap = 0;    // device images + outputs
+  void* hio = nullptr;        size_t hio_cap = 0;    // pinned mirror of dio
+};
+
+namespace {
+
+int grow_dev(void** p, size_t* cap, size_t need) {
+  if (need <= *cap) return DE_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  DE_CUDA(cudaMalloc(p, need));
+  *cap = need;
+  return DE_OK;
+}
+
+int grow_host(void** p, size_t* cap, size_t need) {
+  if (need <= *cap) return DE_OK;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  DE_CUDA(cudaHostAlloc(p, need, cudaHostAllocDefault));
+  *cap = need;
+  return DE_OK;
+}
+
+// Per-pair offsets inside the I/O block: all inputs first, then all outputs, so one
+// copy moves the inputs up and one moves the outputs back.
+struct IoLayout { size_t L, R, disp, margin, conf, cand; };
+struct IoPlan { std::vector<IoLayout> p; size_t in_end = 0, out_begin = 0, end = 0; };
+IoPlan io_plan(const de_pair* hp, int n) {
+  IoPlan plan;
+  plan.p.resize(n);
+  size_t o = 0;
+  for (int i = 0; i < n; ++i) {
+    const size_t WH = size_t(hp[i].W) * hp[i].H;
+    plan.p[i].L = o;  o = align_up(o + WH);
+    plan.p[i].R = o;  o = align_up(o + WH);
+  }
+  plan.in_end = o;
+  plan.out_begin = o;
+  for (int i = 0; i < n; ++i) {
+    const size_t WH = size_t(hp[i].W) * hp[i].H;
+    plan.p[i].disp = o;    o = align_up(o + (hp[i].disp ? WH * 4 : 0));
+    plan.p[i].margin = o;  o = align_up(o + (hp[i].margin ? WH * 4 : 0));
+    plan.p[i].conf = o;    o = align_up(o + (hp[i].conf ? WH : 0));
+    plan.p[i].cand = o;    o = align_up(o + (hp[i].cand ? WH * 24 : 0));
+  }
+  plan.end = o;
+  return plan;
+}
+
+}  // namespace
+
+extern "C" {
+
+int de_ctx_create(const de_cfg* cfg, int device, de_ctx** out) {
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  if (!out) return fail(DE_ERR_ARG, "out is NULL");
+  int ndev = 0;
+  DE_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(DE_ERR_ARG, "no CUDA device %d", device);
+  DE_CUDA(cudaSetDevice(device));
+  de_ctx* c = new de_ctx;
+  c->cfg = *cfg;
+  c->device = device;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
+  *out = c;
+  return DE_OK;
+}
+
+int de_ctx_destroy(de_ctx* c) {
+  if (!c) return DE_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->dws) cudaFree(c->dws);
+  if (c->dio) cudaFree(c->dio);
+  if (c->hio) cudaFreeHost(c->hio);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return DE_OK;
+}
+
+int de_ctx_set_cfg(de_ctx* c, const de_cfg* cfg) {
+  if (!c) return fail(DE_ERR_ARG, "ctx is NULL");
+  int rc = check_cfg(cfg);
+  if (rc) return rc;
+  c->cfg = *cfg;
+  return DE_OK;
+}
+
+int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
+  if (!c || n < 0 || (n > 0 && !hp)) return fail(DE_ERR_ARG, "bad arguments");
+  if (n == 0) return DE_OK;
+  DE_CUDA(cudaSetDevice(c->device));
+  int rc;
+  size_t ws = 0;
+  if ((rc = de_dense_workspace_bytes(&c->cfg, hp, n, &ws))) return rc;
+  const IoPlan plan = io_plan(hp, n);
+  if ((rc = grow_dev(&c->dws, &c->dws_cap, ws))) return rc;
+  if ((rc = grow_dev(&c->dio, &c->dio_cap, plan.end))) return rc;
+  if ((rc = grow_host(&c->hio, &c->hio_cap, plan.end))) return rc;
+  uint8_t* Hb = static_cast<uint8_t*>(c->hio);
+  uint8_t* Db = static_cast<uint8_t*>(c->dio);
+  std::vector<de_pair> dp(n);
+  for (int i = 0; i < n; ++i) {
+    const IoLayout& l = plan.p[i];
+    const size_t WH = size_t(hp[i].W) * hp[i].H;
+    std::memcpy(Hb + l.L, hp[i].L, WH);
+    std::memcpy(Hb + l.R, hp[i].R, WH);
+    dp[i] = hp[i];
+    dp[i].L = Db + l.L;
+    dp[i].R = Db + l.R;
+    dp[i].disp = hp[i].disp ? reinterpret_cast<float*>(Db + l.disp) : nullptr;
+    dp[i].margin = hp[i].margin ? reinterpret_cast<float*>(Db + l.margin) : nullptr;
+    dp[i].conf = hp[i].conf ? Db + l.conf : nullptr;
+    dp[i].cand = hp[i].cand ? reinterpret_cast<float*>(Db + l.cand) : nullptr;
+  }
+  DE_CUDA(cudaMemcpyAsync(Db, Hb, plan.in_end, cudaMemcpyHostToDevice, c->stream));
+  if ((rc = de_dense_dev(&c->cfg, dp.data(), n, c->dws, c->dws_cap, c->stream))) return rc;
+  if (plan.end > plan.out_begin)
+    DE_CUDA(cudaMemcpyAsync(Hb + plan.out_begin, Db + plan.out_begin,
+                            plan.end - plan.out_begin, cudaMemcpyDeviceToHost, c->stream));
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) {
+    const IoLayout& l = plan.p[i];
+    const size_t WH = size_t(hp[i].W) * hp[i].H;
+    if (hp[i].disp) std::memcpy(hp[i].disp, Hb + l.disp, WH * 4);
+    if (hp[i].margin) std::memcpy(hp[i].margin, Hb + l.margin, WH * 4);
+    if (hp[i].conf) std::memcpy(hp[i].conf, Hb + l.conf, WH);
+    if (hp[i].cand) std::memcpy(hp[i].cand, Hb + l.cand, WH * 24);
+  }
+  return DE_OK;
+}
+
+int de_ctx_dense(de_ctx* c, const uint8_t* L, const uint8_t* R, int W, int H, float* disp,
+                 float* margin, uint8_t* conf, float* cand) {
+  de_pair p{};
+  p.L = L; p.R = R; p.W = W; p.H = H; p.dmax = 0;
+  p.disp = disp; p.margin = margin; p.conf = conf; p.cand = cand;
+  return de_ctx_dense_batch(c, &p, 1);
+}
+
+}  // extern "C"

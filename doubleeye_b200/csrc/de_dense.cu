@@ -1,0 +1,759 @@
+// Dense stereo hot path for B200 (sm_100a): census -> graded cost -> four-pass
+// recursive edge-aware filter -> per-pixel top-2 -> MASDA row solve.
+//
+// Arithmetic is the reference's, bit for bit (mayio/doubleeye
+// core/tools/de_dense.cpp, core/include/doubleeye/dense_solve.hpp); the work
+// decomposition is this file's own:
+//
+//   k_census  one thread per pixel over a shared-memory tile with halo, both
+//             images at once; writes a 64-bit census word that also carries the
+//             pixel byte (bits 56..63) when the window fits in 48 bits, so the
+//             cost kernel gets Hamming and absolute-difference inputs in one load,
+//             plus the two Q15 coefficient planes of the left image.
+//   k_rows    one CTA per image row, a thread per PAIR of adjacent disparities
+//             (int16x2 in one 32-bit register): graded score fused with the
+//             horizontal forward pass, then the backward pass, both sequential in
+//             x as integer rounding demands; the row's census words live in
+//             shared memory, the forward result round-trips through L2.
+//   k_cols    one warp per image column, lanes over disparity pairs: vertical
+//             forward pass written in place, vertical backward pass fused with the
+//             top-2 (packed-key warp reduction) and the winner's neighbour costs.
+//   k_solve   one CTA per row: candidate buckets by right pixel, damped max-sum
+//             iterations, belief, and the one-to-one claim done in parallel as a
+//             per-right-pixel arg-max (each pixel claims exactly one right pixel,
+//             so "first in belief order wins" is that arg-max), sub-pixel fit,
+//             reverse-match residuals, confidence.
+//
+// All kernels take the batch descriptor table by value, so one set of launches
+// covers any mix of pair shapes and needs no host-to-device copies (CUDA-graph
+// capturable).  Compiled with --fmad=false: the solve's float arithmetic must not
+// be contracted, to match the reference's x86-64 single-precision results.
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "de_internal.h"
+
+namespace de {
+namespace {
+
+constexpr float kNegBig = -1e30f;
+
+__device__ __forceinline__ int find_pair(const int* prefix, int n, int item) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= item) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One recursive-filter step (core/tools/de_dense.cpp:419): int32 carry, +2^14
+// rounding, arithmetic shift.
+__device__ __forceinline__ int32_t rf_step(int32_t c, int32_t f, int32_t a) {
+  return c + ((a * (f - c) + (1 << 14)) >> 15);
+}
+
+__device__ __forceinline__ uint32_t pack2(int32_t lo, int32_t hi) {
+  return (uint32_t(uint16_t(lo))) | (uint32_t(hi) << 16);
+}
+__device__ __forceinline__ int32_t lo16(uint32_t v) { return int32_t(int16_t(v & 0xFFFFu)); }
+__device__ __forceinline__ int32_t hi16(uint32_t v) { return int32_t(int16_t(v >> 16)); }
+
+// ---------------------------------------------------------------------------------
+// k_census: census words + coefficient planes.
+// core/tools/de_dense.cpp:94-129,186-227 (census), :531-561 (rf_coeffs).
+constexpr int kCTX = 32, kCTY = 8, kMaxHalf = 4;
+
+__global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
+  __shared__ uint8_t sL[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
+  __shared__ uint8_t sR[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
+  __shared__ uint16_t srf[256];
+  const int item = blockIdx.x;
+  const int pi = find_pair(b.pix_prefix, b.n, item);
+  const DevPair& P = b.p[pi];
+  const int W = P.W, H = P.H;
+  const int t = item - b.pix_prefix[pi];
+  const int tilesX = (W + kCTX - 1) / kCTX;
+  const int x0 = (t % tilesX) * kCTX, y0 = (t / tilesX) * kCTY;
+  const int tid = threadIdx.y * kCTX + threadIdx.x;
+  for (int i = tid; i < 256; i += kCTX * kCTY) srf[i] = cfg.rf[i];
+  constexpr int TW = kCTX + 2 * kMaxHalf, TH = kCTY + 2 * kMaxHalf;
+  for (int i = tid; i < TW * TH; i += kCTX * kCTY) {
+    const int ty = i / TW, tx = i % TW;
+    const int gx = x0 + tx - kMaxHalf, gy = y0 + ty - kMaxHalf;
+    const bool in = gx >= 0 && gx < W && gy >= 0 && gy < H;
+    const size_t gi = size_t(gy) * W + gx;
+    sL[ty][tx] = in ? P.L[gi] : 0;
+    sR[ty][tx] = in ? P.R[gi] : 0;
+  }
+  __syncthreads();
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+  if (x >= W || y >= H) return;
+  const int hw = cfg.hw, hh = cfg.hh;
+  const int cx = threadIdx.x + kMaxHalf, cy = threadIdx.y + kMaxHalf;
+  uint64_t wl = 0, wr = 0;
+  if (x >= hw && x < W - hw && y >= hh && y < H - hh) {
+    const uint8_t cl = sL[cy][cx], cr = sR[cy][cx];
+    int bit = 0;
+    for (int dy = -hh; dy <= hh; ++dy)
+      for (int dx = -hw; dx <= hw; ++dx) {
+        if (dx == 0 && dy == 0) continue;
+        wl |= uint64_t(sL[cy + dy][cx + dx] < cl) << bit;
+        wr |= uint64_t(sR[cy + dy][cx + dx] < cr) << bit;
+        ++bit;
+      }
+  }
+  const size_t i = size_t(y) * W + x;
+  if (cfg.packed) {
+    wl |= uint64_t(sL[cy][cx]) << 56;
+    wr |= uint64_t(sR[cy][cx]) << 56;
+  }
+  P.cwL[i] = wl;
+  P.cwR[i] = wr;
+  const int c = sL[cy][cx];
+  P.ax[i] = x > 0 ? srf[abs(c - int(sL[cy][cx - 1]))] : srf[0];
+  P.ay[i] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
+}
+
+// ---------------------------------------------------------------------------------
+// k_rows: graded score + horizontal forward + horizontal backward, one row.
+// Score: core/tools/de_dense.cpp:1224-1233.  Horizontal passes: :411-430.
+//
+// Thread t owns disparities k0 = 2t and k1 = 2t+1 of the row.  The right census
+// word chain k1 needs at x is the one chain k0 used at x-1, so each step loads one
+// right word.  Lanes before their own valid start (x < hw + d) carry exact zeros,
+// which is what the reference's zero-filled plane gives there, so a warp can start
+// at its first lane's start.  Values left of a plane's valid window never reach a
+// valid output (the vertical passes stay within a column and the top-2 masks
+// k > x - hw - dmin), so they are not computed exactly and not needed.
+template <bool PACKED, int TS>
+__device__ __forceinline__ int32_t graded(uint64_t lw, uint64_t rw, const int16_t* stab,
+                                          const uint8_t* sLp, const uint8_t* sRp, int xl,
+                                          int xr) {
+  int h, ad;
+  if (PACKED) {
+    const uint32_t lo = uint32_t(lw) ^ uint32_t(rw);
+    const uint32_t hi = (uint32_t(lw >> 32) ^ uint32_t(rw >> 32));
+    h = __popc(lo) + __popc(hi & 0x00FFFFFFu);
+    ad = abs(int(uint32_t(lw >> 56)) - int(uint32_t(rw >> 56)));
+  } else {
+    h = __popcll(lw ^ rw);
+    ad = abs(int(sLp[xl]) - int(sRp[xr]));
+  }
+  if (TS == 16) ad = min(ad, 15);
+  return stab[h * TS + ad];
+}
+
+template <bool PACKED, int TS>
+__global__ void __launch_bounds__(128) k_rows(DevCfg cfg, Batch b) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int item = blockIdx.x;
+  const int pi = find_pair(b.rows_prefix, b.n, item);
+  const DevPair& P = b.p[pi];
+  const int W = P.W, Dpad = P.Dpad;
+  const int y = cfg.hh + (item - b.rows_prefix[pi]);
+  const int hw = cfg.hw, dmin = cfg.dmin;
+  uint64_t* sL = reinterpret_cast<uint64_t*>(smem);
+  uint64_t* sR = sL + W;
+  uint16_t* sax = reinterpret_cast<uint16_t*>(sR + W);
+  int16_t* stab = reinterpret_cast<int16_t*>(sax + ((W + 7) & ~7));
+  uint8_t* sLp = reinterpret_cast<uint8_t*>(stab + 66 * TS);
+  uint8_t* sRp = sLp + W;
+  const size_t row = size_t(y) * W;
+  for (int i = threadIdx.x; i < W; i += blockDim.x) {
+    sL[i] = P.cwL[row + i];
+    sR[i] = P.cwR[row + i];
+    sax[i] = P.ax[row + i];
+    if (!PACKED) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
+  }
+  for (int i = threadIdx.x; i < 66 * TS; i += blockDim.x) {
+    const int h = i / TS, m = i % TS;
+    stab[i] = int16_t((int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10);
+  }
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (2 * t >= Dpad) return;
+  const int d0 = dmin + 2 * t;
+  const int xw = hw + dmin + 2 * (t & ~31);          // first lane's start in this warp
+  const int xend = W - hw;                            // scores are 0 from here on
+  uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * Dpad) + t;
+  const size_t xs = size_t(Dpad) >> 1;                // x stride in 32-bit words
+  int32_t f0 = 0, f1 = 0;
+  // previous step's right word = chain k1's word at the first step
+  uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;
+  int x = xw;
+  // ramp: lanes may not have reached their own valid start yet
+  const int xramp = min(xend, xw + 64);
+  for (; x < xramp; ++x) {
+    const int32_t a = sax[x];
+    const uint64_t lw = sL[x];
+    int32_t v0 = 0, v1 = 0;
+    uint64_t rw = 0;
+    if (x - d0 >= hw) {
+      rw = sR[x - d0];
+      v0 = graded<PACKED, TS>(lw, rw, stab, sLp, sRp, x, x - d0);
+    }
+    if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS>(lw, rprev, stab, sLp, sRp, x, x - d0 - 1);
+    rprev = rw;
+    f0 = rf_step(v0, f0, a);
+    f1 = rf_step(v1, f1, a);
+    out[x * xs] = pack2(f0, f1);
+  }
+  // main: every chain in the warp is inside its window
+#pragma unroll 4
+  for (; x < xend; ++x) {
+    const int32_t a = sax[x];
+    const uint64_t lw = sL[x];
+    const uint64_t rw = sR[x - d0];
+    const int32_t v0 = graded<PACKED, TS>(lw, rw, stab, sLp, sRp, x, x - d0);
+    const int32_t v1 = graded<PACKED, TS>(lw, rprev, stab, sLp, sRp, x, x - d0 - 1);
+    rprev = rw;
+    f0 = rf_step(v0, f0, a);
+    f1 = rf_step(v1, f1, a);
+    out[x * xs] = pack2(f0, f1);
+  }
+  // tail: right border, score 0
+  for (; x < W; ++x) {
+    const int32_t a = sax[x];
+    f0 = rf_step(0, f0, a);
+    f1 = rf_step(0, f1, a);
+    out[x * xs] = pack2(f0, f1);
+  }
+  // backward: seed with the forward value at W-1 (already stored), coefficient at x+1
+  int32_t g0 = f0, g1 = f1;
+  const int xlo = xw;
+  x = W - 2;
+  constexpr int PF = 8;
+  uint32_t ring[PF];
+#pragma unroll
+  for (int j = 0; j < PF; ++j) ring[j] = (x - j >= xlo) ? out[(x - j) * xs] : 0u;
+  while (x >= xlo) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int xx = x - j;
+      if (xx >= xlo) {
+        const uint32_t c = ring[j];
+        const int32_t a = sax[xx + 1];
+        g0 = rf_step(lo16(c), g0, a);
+        g1 = rf_step(hi16(c), g1, a);
+        ring[j] = (xx - PF >= xlo) ? out[(xx - PF) * xs] : 0u;
+        out[xx * xs] = pack2(g0, g1);
+      }
+    }
+    x -= PF;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// k_cols: vertical forward (in place), vertical backward + top-2 + neighbours.
+// Vertical passes: core/tools/de_dense.cpp:490-507.  Top-2 semantics: :1276-1292
+// (ascending k, strictly greater, ties keep the smaller k), sub-pixel neighbour
+// capture :1276-1285.  The packed key ((v + 32768) << 8 | (255 - k)) makes the
+// reduction order-independent, so a shuffle tree reproduces the sequential scan.
+template <int G>
+__global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= b.cols_prefix[b.n]) return;
+  const int pi = find_pair(b.cols_prefix, b.n, warp);
+  const DevPair& P = b.p[pi];
+  const int W = P.W, H = P.H, D = P.D, Dpad = P.Dpad;
+  const int hw = cfg.hw, hh = cfg.hh, dmin = cfg.dmin;
+  const int x = hw + dmin + (warp - b.cols_prefix[pi]);
+  const int kmax = min(D - 1, x - hw - dmin);
+  const int Gp = Dpad >> 6;                          // this pair's groups (<= G)
+  uint32_t* col = reinterpret_cast<uint32_t*>(P.vol + size_t(x) * Dpad) + lane;
+  const size_t rs = size_t(W) * Dpad / 2;           // row stride, 32-bit words
+  const uint16_t* ay = P.ay + x;
+  int32_t p0[G], p1[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) { p0[g] = 0; p1[g] = 0; }
+  // forward: rows < hh are zero, rows >= H-hh have zero input
+  const int yin = H - hh;
+  constexpr int PF = 4;
+  uint32_t ring[PF][G];
+#pragma unroll
+  for (int j = 0; j < PF; ++j)
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      ring[j][g] = (g < Gp && hh + j < yin) ? col[size_t(hh + j) * rs + g * 32] : 0u;
+  for (int y0 = hh; y0 < H; y0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int y = y0 + j;
+      if (y < H) {
+        const int32_t a = ay[size_t(y) * W];
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          if (g >= Gp) break;
+          const uint32_t c = ring[j][g];
+          ring[j][g] = (y + PF < yin) ? col[size_t(y + PF) * rs + g * 32] : 0u;
+          p0[g] = rf_step(lo16(c), p0[g], a);
+          p1[g] = rf_step(hi16(c), p1[g], a);
+          col[size_t(y) * rs + g * 32] = pack2(p0[g], p1[g]);
+        }
+      }
+    }
+  }
+  // backward from H-1 (its value is the forward value), coefficient at y+1
+  uint32_t* key0 = P.key0 + x;
+  uint32_t* key1 = P.key1 + x;
+  uint32_t* nbp = P.nb + x;
+  uint32_t* rkey = P.rkey;
+#pragma unroll
+  for (int j = 0; j < PF; ++j)
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      ring[j][g] = (g < Gp && H - 2 - j >= hh) ? col[size_t(H - 2 - j) * rs + g * 32] : 0u;
+  for (int y0 = H - 2; y0 >= hh; y0 -= PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      const int y = y0 - j;
+      if (y >= hh) {
+        const int32_t a = ay[size_t(y + 1) * W];
+        uint32_t pk0 = 0, pk1 = 0;
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          if (g >= Gp) break;
+          const uint32_t c = ring[j][g];
+          ring[j][g] = (y - PF >= hh) ? col[size_t(y - PF) * rs + g * 32] : 0u;
+          p0[g] = rf_step(lo16(c), p0[g], a);
+          p1[g] = rf_step(hi16(c), p1[g], a);
+          const int k2 = g * 64 + lane * 2;
+          if (k2 <= kmax) {
+            const uint32_t c0 = (uint32_t(p0[g] + 32768) << 8) | uint32_t(255 - k2);
+            if (c0 > pk0) { pk1 = pk0; pk0 = c0; } else if (c0 > pk1) { pk1 = c0; }
+          }
+          if (k2 + 1 <= kmax) {
+            const uint32_t c1 = (uint32_t(p1[g] + 32768) << 8) | uint32_t(255 - k2 - 1);
+            if (c1 > pk0) { pk1 = pk0; pk0 = c1; } else if (c1 > pk1) { pk1 = c1; }
+          }
+        }
+        if (y < H - hh) {
+          if (rkey) {
+            const size_t rowo = size_t(y) * W + x - dmin;
+#pragma unroll
+            for (int g = 0; g < G; ++g) {
+              const int k2 = g * 64 + lane * 2;
+              if (k2 <= kmax)
+                atomicMax(rkey + rowo - k2, (uint32_t(p0[g] + 32768) << 8) | uint32_t(255 - k2));
+              if (k2 + 1 <= kmax)
+                atomicMax(rkey + rowo - k2 - 1,
+                          (uint32_t(p1[g] + 32768) << 8) | uint32_t(255 - k2 - 1));
+            }
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            const uint32_t o0 = __shfl_down_sync(0xffffffffu, pk0, off);
+            const uint32_t o1 = __shfl_down_sync(0xffffffffu, pk1, off);
+            if (o0 > pk0) { pk1 = pk0 > o1 ? pk0 : o1; pk0 = o0; }
+            else if (o0 > pk1) { pk1 = o0; }
+          }
+          const uint32_t w0 = __shfl_sync(0xffffffffu, pk0, 0);
+          const int kw = w0 ? 255 - int(w0 & 255u) : -1;
+          const int km = kw - 1, kp = kw + 1;
+          int32_t mym = -32768, myp = -32768;
+#pragma unroll
+          for (int g = 0; g < G; ++g) {
+            const int k2 = g * 64 + lane * 2;
+            if (k2 <= kmax) { if (k2 == km) mym = p0[g]; if (k2 == kp) myp = p0[g]; }
+            if (k2 + 1 <= kmax) { if (k2 + 1 == km) mym = p1[g]; if (k2 + 1 == kp) myp = p1[g]; }
+          }
+          const int32_t vm = __shfl_sync(0xffffffffu, mym, (km & 63) >> 1);
+          const int32_t vp = __shfl_sync(0xffffffffu, myp, (kp & 63) >> 1);
+          if (lane == 0) {
+            const size_t i = size_t(y) * W;
+            key0[i] = pk0;
+            key1[i] = pk1;
+            const int32_t nm = (kw >= 0 && km >= 0) ? vm : -32768;
+            const int32_t np = (kw >= 0) ? vp : -32768;
+            nbp[i] = pack2(nm, np);
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// k_solve: the row solve, core/include/doubleeye/dense_solve.hpp:213-452 (K = 2,
+// candidates from the cost stage), plus the --out-conf planes and the confidence
+// (:158-171).  One CTA per row; shared-memory working set ~53 bytes per pixel.
+constexpr int kSolveThreads = 256;
+
+__device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }
+__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }
+
+__device__ float confidence_dev(float s1, float s2, float lambda, float lrc, float tol) {
+  if (!(s1 > -1e29f)) return 0.f;
+  const float alt = (s2 > -1e29f) ? fmax_ref(s2, lambda) : lambda;
+  const float x = logf(fmax_ref((1.f - alt) / fmax_ref(1.f - s1, 1e-6f), 1e-6f));
+  const float logit = 0.692684f + 7.936751f * x;
+  const float p = 1.f / (1.f + expf(-fmax_ref(-30.f, fmin_ref(30.f, logit))));
+  return (lrc > tol) ? fmin_ref(p, 0.35f) : p;
+}
+
+__device__ __forceinline__ void block_excl_scan(int* a, int n, int* warp_sums) {
+  // exclusive scan of a[0..n) in place, a[n] = total; 256 threads, contiguous chunks
+  const int tid = threadIdx.x;
+  const int per = (n + kSolveThreads - 1) / kSolveThreads;
+  const int lo = min(n, tid * per), hi = min(n, lo + per);
+  int s = 0;
+  for (int i = lo; i < hi; ++i) s += a[i];
+  // inclusive warp scan of s
+  const int lane = tid & 31, w = tid >> 5;
+  int v = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += u;
+  }
+  if (lane == 31) warp_sums[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    int ws = lane < (kSolveThreads / 32) ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int u = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += u;
+    }
+    if (lane < kSolveThreads / 32) warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  int run = v - s + (w > 0 ? warp_sums[w - 1] : 0);
+  for (int i = lo; i < hi; ++i) { const int c = a[i]; a[i] = run; run += c; }
+  if (tid == kSolveThreads - 1) a[n] = run;
+  __syncthreads();
+}
+
+template <bool REF_LAYOUT>
+__global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int item = blockIdx.x;
+  const int pi = find_pair(b.solve_prefix, b.n, item);
+  const DevPair& P = b.p[pi];
+  const int W = P.W, H = P.H;
+  const int y = item - b.solve_prefix[pi];
+  const int dmin = cfg.dmin, hw = cfg.hw, hh = cfg.hh;
+  const float lambda = cfg.lambda, gamma = cfg.gamma, damping = cfg.damping, keep = cfg.keep;
+  float* s_cs = reinterpret_cast<float*>(smem);          // [2W]
+  float* s_beta = s_cs + 2 * W;                           // [2W]
+  float* s_rho = s_beta + 2 * W;                          // [2W]
+  float* s_best = s_rho + 2 * W;                          // [W]
+  float* s_margin = s_best + W;                           // [W]
+  int* s_start = reinterpret_cast<int*>(s_margin + W);    // [W+1]
+  int* s_cur = s_start + W + 1;                           // [W]
+  int16_t* s_items = reinterpret_cast<int16_t*>(s_cur + W);   // [2W]
+  int16_t* s_cd = s_items + 2 * W;                        // [2W]
+  int16_t* s_rev = s_cd + 2 * W;                          // [W]
+  int8_t* s_cn = reinterpret_cast<int8_t*>(s_rev + W);    // [W]
+  int8_t* s_bestj = s_cn + W;                             // [W]
+  uint8_t* s_win = reinterpret_cast<uint8_t*>(s_bestj + W);  // [W]
+  __shared__ int warp_sums[kSolveThreads / 32];
+  const int tid = threadIdx.x;
+  const bool row_ok = y >= hh && y < H - hh;
+  const size_t row = size_t(y) * W;
+  const float q = 1.f / 16384.f;
+
+  // 1. candidates + margin (dense_solve.hpp:263-268)
+  for (int x = tid; x < W; x += kSolveThreads) {
+    int n = 0;
+    float c0 = kNegBig, c1 = kNegBig;
+    int k0 = -1, k1 = -1;
+    if (REF_LAYOUT) {
+      n = P.ref_cn[row + x];
+      if (n > 0) { c0 = P.ref_cs[2 * (row + x)]; k0 = P.ref_cd[2 * (row + x)]; }
+      if (n > 1) { c1 = P.ref_cs[2 * (row + x) + 1]; k1 = P.ref_cd[2 * (row + x) + 1]; }
+    } else if (row_ok && x >= hw + dmin && x < W - hw) {
+      const uint32_t a = P.key0[row + x], bb = P.key1[row + x];
+      if (a) { c0 = float(int32_t(a >> 8) - 32768) * q; k0 = 255 - int(a & 255u); n = 1; }
+      if (bb) { c1 = float(int32_t(bb >> 8) - 32768) * q; k1 = 255 - int(bb & 255u); n = 2; }
+    }
+    s_cs[2 * x] = c0; s_cs[2 * x + 1] = c1;
+    s_cd[2 * x] = int16_t(k0); s_cd[2 * x + 1] = int16_t(k1);
+    s_cn[x] = int8_t(n);
+    const float alt = (n < 2) ? lambda : fmax_ref(c1, lambda);
+    const float m = (n == 0) ? 0.f : c0 - alt;
+    s_margin[x] = m;
+    if (P.margin) P.margin[row + x] = m;
+    s_start[x] = 0;
+    s_beta[2 * x] = s_beta[2 * x + 1] = 0.f;
+    s_rho[2 * x] = s_rho[2 * x + 1] = 0.f;
+    s_win[x] = 0;
+  }
+  __syncthreads();
+  // 2. claimant buckets by right pixel (:270-284); order inside a bucket is free
+  for (int x = tid; x < W; x += kSolveThreads)
+    for (int j = 0; j < s_cn[x]; ++j) {
+      const int xr = x - (dmin + s_cd[2 * x + j]);
+      if (xr >= 0 && xr < W) atomicAdd(&s_start[xr], 1);
+    }
+  __syncthreads();
+  block_excl_scan(s_start, W, warp_sums);
+  for (int xr = tid; xr < W; xr += kSolveThreads) s_cur[xr] = s_start[xr];
+  __syncthreads();
+  for (int x = tid; x < W; x += kSolveThreads)
+    for (int j = 0; j < s_cn[x]; ++j) {
+      const int xr = x - (dmin + s_cd[2 * x + j]);
+      if (xr >= 0 && xr < W) s_items[atomicAdd(&s_cur[xr], 1)] = int16_t(2 * x + j);
+    }
+  __syncthreads();
+  // 3. reverse match over surviving candidates (:303-313): first maximum in x order
+  for (int xr = tid; xr < W; xr += kSolveThreads) {
+    int bd = -1, bi = 1 << 30;
+    float bv = kNegBig;
+    for (int p = s_start[xr]; p < s_start[xr + 1]; ++p) {
+      const int idx = s_items[p];
+      const float v = s_cs[idx];
+      if (v > bv || (v == bv && idx < bi)) { bv = v; bd = s_cd[idx]; bi = idx; }
+    }
+    s_rev[xr] = int16_t(bd);
+  }
+  // 4. damped max-sum iterations (:318-341)
+  for (int it = 0; it < cfg.iters; ++it) {
+    __syncthreads();
+    for (int x = tid; x < W; x += kSolveThreads) {
+      const int n = s_cn[x];
+      for (int j = 0; j < n; ++j) {
+        const float ex = (n == 2) ? s_beta[2 * x + 1 - j] : kNegBig;
+        const float tgt = s_cs[2 * x + j] - fmax_ref(lambda, ex);
+        s_rho[2 * x + j] = keep * tgt + damping * s_rho[2 * x + j];
+      }
+    }
+    __syncthreads();
+    for (int xr = tid; xr < W; xr += kSolveThreads) {
+      const int lo = s_start[xr], hi = s_start[xr + 1];
+      if (hi <= lo) continue;
+      float b1 = kNegBig, b2 = kNegBig;
+      int i1 = -1;
+      for (int p = lo; p < hi; ++p) {
+        const float v = s_rho[s_items[p]];
+        if (v > b1) { b2 = b1; b1 = v; i1 = p; } else if (v > b2) { b2 = v; }
+      }
+      for (int p = lo; p < hi; ++p) {
+        const int idx = s_items[p];
+        const float ex = (p == i1) ? b2 : b1;
+        s_beta[idx] = keep * (s_cs[idx] - fmax_ref(gamma, ex)) + damping * s_beta[idx];
+      }
+    }
+  }
+  __syncthreads();
+  // 5. belief (:343-358)
+  for (int x = tid; x < W; x += kSolveThreads) {
+    float best = kNegBig;
+    int bj = -1;
+    for (int j = 0; j < s_cn[x]; ++j) {
+      const float c = s_cs[2 * x + j];
+      if (c <= lambda) continue;
+      const float bel = (cfg.iters > 0) ? (s_beta[2 * x + j] + s_rho[2 * x + j] - c) : c;
+      if (bel > best) { best = bel; bj = j; }
+    }
+    // gates (:364-374) fold into eligibility
+    if (bj >= 0 && cfg.min_margin > 0.f && s_margin[x] < cfg.min_margin) bj = -1;
+    if (bj >= 0 && cfg.min_ratio > 0.f) {
+      const float s2 = (s_cn[x] > 1) ? fmax_ref(s_cs[2 * x + 1], lambda) : lambda;
+      const float c1 = fmax_ref(1.f - s_cs[2 * x], 1e-6f);
+      if ((1.f - s2) / c1 < cfg.min_ratio) bj = -1;
+    }
+    s_best[x] = best;
+    s_bestj[x] = int8_t(bj);
+  }
+  __syncthreads();
+  // 6. one-to-one claim (:359-378): each eligible pixel claims exactly one right
+  //    pixel, so the sequential greedy pass equals, per right pixel, the claimant
+  //    first in (belief desc, x asc) order.
+  for (int xr = tid; xr < W; xr += kSolveThreads) {
+    int wx = -1;
+    float wb = 0.f;
+    for (int p = s_start[xr]; p < s_start[xr + 1]; ++p) {
+      const int idx = s_items[p];
+      const int x = idx >> 1, j = idx & 1;
+      if (s_bestj[x] != j) continue;
+      const float bv = s_best[x];
+      if (wx < 0 || bv > wb || (bv == wb && x < wx)) { wx = x; wb = bv; }
+    }
+    if (wx >= 0) s_win[wx] = 1;
+  }
+  __syncthreads();
+  // 7. outputs: disparity with sub-pixel fit (:380-434), reverse-match residuals
+  //    (:442-451, core/tools/de_dense.cpp:1581-1597), candidate planes, confidence
+  const size_t WH = size_t(W) * H;
+  for (int x = tid; x < W; x += kSolveThreads) {
+    float dl = __int_as_float(0x7fc00000);
+    const int n = s_cn[x];
+    if (s_win[x]) {
+      const int j = s_bestj[x];
+      const int d = dmin + s_cd[2 * x + j];
+      float off = 0.f;
+      if (cfg.subpixel && j == 0) {
+        int32_t m16 = -32768, p16 = -32768;
+        if (REF_LAYOUT) {
+          if (P.ref_cnb) { m16 = P.ref_cnb[2 * (row + x)]; p16 = P.ref_cnb[2 * (row + x) + 1]; }
+        } else {
+          const uint32_t nb = P.nb[row + x];
+          m16 = lo16(nb); p16 = hi16(nb);
+        }
+        const float c0 = s_cs[2 * x];
+        const float cm = (m16 == -32768) ? kNegBig : float(m16) * q;
+        const float cp = (p16 == -32768) ? kNegBig : float(p16) * q;
+        if (cm > -1e29f && cp > -1e29f) {
+          if (cfg.fit_eq) {
+            const float lower = cm < cp ? cm : cp;
+            const float den = c0 - lower;
+            if (den > 1e-6f) { off = 0.5f * (cp - cm) / den; off = off > 0.5f ? 0.5f : (off < -0.5f ? -0.5f : off); }
+          } else {
+            const float den = 2.f * c0 - cm - cp;
+            if (den > 1e-6f) { off = 0.5f * (cp - cm) / den; off = off > 0.5f ? 0.5f : (off < -0.5f ? -0.5f : off); }
+          }
+        }
+      }
+      dl = float(d) + off;
+    }
+    if (P.disp) P.disp[row + x] = dl;
+    float lrc2 = __int_as_float(0x7fc00000);
+    float lrc = cfg.lrc ? __int_as_float(0x7fc00000) : kNegBig;
+    if (dl == dl) {
+      const int xr = x - int(lroundf(dl));
+      if (xr >= 0 && xr < W) {
+        if (s_rev[xr] >= 0) lrc2 = fabsf(dl - float(dmin + s_rev[xr]));
+        if (cfg.lrc && P.rkey) {
+          const uint32_t rk = P.rkey[row + xr];
+          if (rk) lrc = fabsf(dl - float(dmin + 255 - int(rk & 255u)));
+        }
+      }
+    }
+    if (P.lrc2) P.lrc2[row + x] = lrc2;
+    const float s1 = n > 0 ? s_cs[2 * x] : kNegBig;
+    const float s2 = n > 1 ? s_cs[2 * x + 1] : kNegBig;
+    if (P.cand) {
+      P.cand[row + x] = s1;
+      P.cand[WH + row + x] = s2;
+      P.cand[2 * WH + row + x] = n > 0 ? float(dmin + s_cd[2 * x]) : kNegBig;
+      P.cand[3 * WH + row + x] = n > 1 ? float(dmin + s_cd[2 * x + 1]) : kNegBig;
+      P.cand[4 * WH + row + x] = lrc;
+      P.cand[5 * WH + row + x] = lrc2;
+    }
+    if (P.conf) {
+      uint8_t cv = 0;
+      if (dl == dl)
+        cv = uint8_t(lroundf(confidence_dev(s1, s2, lambda, (lrc2 == lrc2) ? lrc2 : 0.f, 1.f) * 255.f));
+      P.conf[row + x] = cv;
+    }
+  }
+}
+
+// Reference-layout candidates (core/tools/de_dense_cuda.cu:384-390) from packed keys.
+__global__ void k_export(DevCfg cfg, Batch b) {
+  const int item = blockIdx.x;
+  const int pi = find_pair(b.solve_prefix, b.n, item);
+  const DevPair& P = b.p[pi];
+  const int W = P.W, H = P.H, y = item - b.solve_prefix[pi];
+  const bool row_ok = y >= cfg.hh && y < H - cfg.hh;
+  const float q = 1.f / 16384.f;
+  for (int x = threadIdx.x; x < W; x += blockDim.x) {
+    const size_t i = size_t(y) * W + x;
+    uint32_t a = 0, bb = 0, nb = 0x80008000u;
+    if (row_ok && x >= cfg.hw + cfg.dmin && x < W - cfg.hw) { a = P.key0[i]; bb = P.key1[i]; nb = P.nb[i]; }
+    int n = 0;
+    P.ref_cs[2 * i] = kNegBig; P.ref_cs[2 * i + 1] = kNegBig;
+    P.ref_cd[2 * i] = -1; P.ref_cd[2 * i + 1] = -1;
+    if (a) { P.ref_cs[2 * i] = float(int32_t(a >> 8) - 32768) * q; P.ref_cd[2 * i] = 255 - int(a & 255u); n = 1; }
+    if (bb) { P.ref_cs[2 * i + 1] = float(int32_t(bb >> 8) - 32768) * q; P.ref_cd[2 * i + 1] = 255 - int(bb & 255u); n = 2; }
+    P.ref_cn[i] = n;
+    if (P.ref_cnb) {
+      P.ref_cnb[2 * i] = int16_t(n && cfg.subpixel ? lo16(nb) : -32768);
+      P.ref_cnb[2 * i + 1] = int16_t(n && cfg.subpixel ? hi16(nb) : -32768);
+    }
+  }
+}
+
+size_t rows_smem(int W, int TS, bool packed) {
+  size_t s = size_t(W) * 16 + size_t((W + 7) & ~7) * 2 + size_t(66) * TS * 2;
+  if (!packed) s += size_t(W) * 2;
+  return (s + 15) & ~size_t(15);
+}
+
+size_t solve_smem(int W) { return size_t(W) * 53 + 64; }
+
+template <typename K>
+cudaError_t set_smem(K kernel, size_t bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
+}
+
+}  // namespace
+
+cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  const int tiles = b.pix_prefix[b.n];
+  if (tiles == 0) return cudaSuccess;
+  k_census<<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  const int items = b.rows_prefix[b.n];
+  if (items == 0) return cudaSuccess;
+  int maxW = 0;
+  for (int i = 0; i < b.n; ++i) maxW = maxW > b.p[i].W ? maxW : b.p[i].W;
+  const int TS = cfg.trunc < 16 ? 16 : 256;
+  const size_t sm = rows_smem(maxW, TS, cfg.packed != 0);
+  const int threads = b.maxDpad / 2;
+  cudaError_t e;
+  if (cfg.packed) {
+    if (TS == 16) {
+      if ((e = set_smem(k_rows<true, 16>, sm)) != cudaSuccess) return e;
+      k_rows<true, 16><<<items, threads, sm, s>>>(cfg, b);
+    } else {
+      if ((e = set_smem(k_rows<true, 256>, sm)) != cudaSuccess) return e;
+      k_rows<true, 256><<<items, threads, sm, s>>>(cfg, b);
+    }
+  } else {
+    if (TS == 16) {
+      if ((e = set_smem(k_rows<false, 16>, sm)) != cudaSuccess) return e;
+      k_rows<false, 16><<<items, threads, sm, s>>>(cfg, b);
+    } else {
+      if ((e = set_smem(k_rows<false, 256>, sm)) != cudaSuccess) return e;
+      k_rows<false, 256><<<items, threads, sm, s>>>(cfg, b);
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  const int warps = b.cols_prefix[b.n];
+  if (warps == 0) return cudaSuccess;
+  const int blocks = (warps * 32 + 255) / 256;
+  switch (b.maxDpad / 64) {
+    case 1: k_cols<1><<<blocks, 256, 0, s>>>(cfg, b); break;
+    case 2: k_cols<2><<<blocks, 256, 0, s>>>(cfg, b); break;
+    case 3: k_cols<3><<<blocks, 256, 0, s>>>(cfg, b); break;
+    default: k_cols<4><<<blocks, 256, 0, s>>>(cfg, b); break;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref, cudaStream_t s) {
+  const int items = b.solve_prefix[b.n];
+  if (items == 0) return cudaSuccess;
+  int maxW = 0;
+  for (int i = 0; i < b.n; ++i) maxW = maxW > b.p[i].W ? maxW : b.p[i].W;
+  const size_t sm = solve_smem(maxW);
+  cudaError_t e;
+  if (from_ref) {
+    if ((e = set_smem(k_solve<true>, sm)) != cudaSuccess) return e;
+    k_solve<true><<<items, kSolveThreads, sm, s>>>(cfg, b);
+  } else {
+    if ((e = set_smem(k_solve<false>, sm)) != cudaSuccess) return e;
+    k_solve<false><<<items, kSolveThreads, sm, s>>>(cfg, b);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  const int items = b.solve_prefix[b.n];
+  if (items == 0) return cudaSuccess;
+  k_export<<<items, 256, 0, s>>>(cfg, b);
+  return cudaGetLastError();
+}
+
+}  // namespace de

@@ -1,0 +1,83 @@
+// Internal interfaces between the C ABI (de_capi.cu) and the kernels
+// (de_dense.cu).  Not installed; include/doubleeye_b200.h is the public surface.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "../../include/doubleeye_b200.h"
+
+namespace de {
+
+// Largest batch one launch set carries; the descriptor table travels as a kernel
+// parameter (no host-to-device copy, so launches are graph-capturable and need no
+// allocation).  Bigger batches are split by the host.
+constexpr int kMaxBatch = 64;
+constexpr int kMaxW = 4096;    // row kernel keeps two census rows of W in shared memory
+constexpr int kMaxH = 8192;
+
+// Per-pair device layout.  Every pointer is device memory.
+struct DevPair {
+  const uint8_t* L;
+  const uint8_t* R;
+  uint64_t* cwL;       // census word | pixel << 56 (7x7) or census only (wider windows)
+  uint64_t* cwR;
+  uint16_t* ax;        // Q15 filter coefficients of L, x direction
+  uint16_t* ay;        // ... y direction
+  int16_t* vol;        // [H][W][Dpad] filtered cost, int16 (Q14)
+  uint32_t* key0;      // packed top-2 keys, (v + 32768) << 8 | (255 - k); 0 = empty
+  uint32_t* key1;
+  uint32_t* nb;        // winner's neighbour costs, lo16 = k*-1, hi16 = k*+1 (-32768 none)
+  uint32_t* rkey;      // exact reverse match per right pixel (cfg.lrc), may be null
+  float* disp;         // outputs, any may be null
+  float* margin;
+  uint8_t* conf;
+  float* cand;         // 6 planes s1,s2,d1,d2,lrc,lrc2
+  float* lrc2;         // the lrc2 plane alone (stage entry point), may be null
+  // reference-layout candidates for the stage entry points (null otherwise)
+  float* ref_cs;
+  int* ref_cd;
+  int* ref_cn;
+  int16_t* ref_cnb;
+  int W, H, D, Dpad;
+};
+
+// Arithmetic configuration, precomputed on the host from de_cfg.
+struct DevCfg {
+  int dmin, iters, hw, hh;
+  int wq;              // AD weight in 1/1024
+  int trunc;           // AD truncation
+  int packed;          // census words carry the pixel byte (window <= 48 bits)
+  int subpixel, fit_eq, lrc;
+  float lambda, gamma, damping, keep, min_margin, min_ratio;
+  int16_t tbl[66];     // Q14 census score per Hamming distance
+  int16_t adt[256];    // Q14 truncated-absolute-difference score
+  uint16_t rf[256];    // Q15 filter coefficient per byte difference
+};
+
+struct Batch {
+  int n;
+  int maxDpad;
+  int rows_prefix[kMaxBatch + 1];   // row-kernel work items (rows in [hh, H-hh))
+  int cols_prefix[kMaxBatch + 1];   // column-kernel work items (cols with candidates)
+  int solve_prefix[kMaxBatch + 1];  // solve work items (all rows)
+  int pix_prefix[kMaxBatch + 1];    // census tiles
+  DevPair p[kMaxBatch];
+};
+
+// Host-side preparation (de_capi.cu).
+void make_dev_cfg(const de_cfg& c, DevCfg* out);
+size_t pair_workspace_bytes(int W, int H, int D, bool lrc);
+void carve_pair(DevPair* p, void* ws, int W, int H, int D, bool lrc);
+
+// Launchers (de_dense.cu).  All enqueue on `stream` and return the launch status.
+cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s);
+cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s);
+cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s);
+cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref_layout,
+                         cudaStream_t s);
+cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
+
+}  // namespace de

@@ -1,0 +1,246 @@
+"""Dense MASDA stereo on the GPU: the host-side mirror of the reference's dense tools.
+
+Reference call surface (mayio/doubleeye):
+  ``run_dense`` (core/tools/de_dense.cpp:738) -> ``run_dense`` here (host arrays, one
+  or many pairs), ``DenseMatcher`` (device tensors, caller stream, reusable workspace);
+  ``Cfg`` (core/include/doubleeye/dense_solve.hpp:19-97) -> ``Cfg``; the --out-conf
+  planes s1,s2,d1,d2,lrc,lrc2 (core/tools/de_dense.cpp:727-737) -> ``cand``.
+
+Every call goes through the C ABI into the sm_100a kernels; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import threading
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import DeCfg, DePair, check, lib
+
+CAND_PLANES = ("s1", "s2", "d1", "d2", "lrc", "lrc2")
+
+
+def Cfg(**overrides) -> DeCfg:
+    """A de_cfg with the reference defaults (dmin 1, dmax 60, iters 0, sigma_s 8,
+    sigma_r 0.2, ad 0.15, ad_trunc 10, lambda = gamma = -0.1, damping 0.4, sub-pixel
+    equiangular fit, 7x7 census) and any field overridden by keyword (``lambda_`` or
+    ``lambda`` for the clutter cost)."""
+    c = DeCfg()
+    lib().de_cfg_default(C.byref(c))
+    for k, v in overrides.items():
+        k = "lambda_" if k == "lambda" else k
+        if not hasattr(c, k):
+            raise TypeError(f"unknown de_cfg field {k!r}")
+        setattr(c, k, v)
+    return c
+
+
+def cfg_dict(c: DeCfg) -> dict:
+    return {f: getattr(c, f) for f, _ in c._fields_}
+
+
+@dataclasses.dataclass
+class DenseResult:
+    disp: np.ndarray            # f32 (H, W), NaN where the matcher declined
+    margin: np.ndarray          # f32 (H, W)
+    conf: np.ndarray            # u8 (H, W)
+    cand: Optional[np.ndarray]  # f32 (6, H, W): s1, s2, d1, d2, lrc, lrc2
+
+
+class _Ctx:
+    """A de_ctx (host-pointer entry points) per thread and device."""
+    _tls = threading.local()
+
+    @classmethod
+    def get(cls, device: int = 0):
+        cache = getattr(cls._tls, "ctx", None)
+        if cache is None:
+            cache = cls._tls.ctx = {}
+        if device not in cache:
+            h = C.c_void_p()
+            check(lib().de_ctx_create(C.byref(Cfg()), device, C.byref(h)))
+            cache[device] = h
+        return cache[device]
+
+
+def _u8(a) -> np.ndarray:
+    a = np.ascontiguousarray(a)
+    if a.dtype != np.uint8 or a.ndim != 2:
+        raise ValueError("images must be 2-D uint8")
+    return a
+
+
+def run_dense(left, right, cfg: Optional[DeCfg] = None, *, want_cand: bool = True,
+              device: int = 0) -> DenseResult:
+    """One pair, host arrays in and out (uploads, runs every stage, downloads)."""
+    return run_dense_batch([(left, right)], cfg, want_cand=want_cand, device=device)[0]
+
+
+def run_dense_batch(pairs: Sequence, cfg: Optional[DeCfg] = None, *, want_cand=False,
+                    device: int = 0) -> list[DenseResult]:
+    """Many pairs of any sizes in one batched launch set.  ``pairs`` holds
+    (left, right) or (left, right, dmax) tuples; dmax defaults to the cfg's."""
+    cfg = cfg or Cfg()
+    ctx = _Ctx.get(device)
+    check(lib().de_ctx_set_cfg(ctx, C.byref(cfg)))
+    keep, outs = [], []
+    arr = (DePair * len(pairs))()
+    for i, pr in enumerate(pairs):
+        L, R = _u8(pr[0]), _u8(pr[1])
+        if L.shape != R.shape:
+            raise ValueError("left and right differ in shape")
+        H, W = L.shape
+        res = DenseResult(np.empty((H, W), np.float32), np.empty((H, W), np.float32),
+                          np.empty((H, W), np.uint8),
+                          np.empty((6, H, W), np.float32) if want_cand else None)
+        keep += [L, R]
+        outs.append(res)
+        arr[i] = DePair(L.ctypes.data, R.ctypes.data, W, H, int(pr[2]) if len(pr) > 2 else 0,
+                        res.disp.ctypes.data, res.margin.ctypes.data, res.conf.ctypes.data,
+                        res.cand.ctypes.data if want_cand else None)
+    check(lib().de_ctx_dense_batch(ctx, arr, len(pairs)))
+    return outs
+
+
+# --------------------------------------------------------------------------------------
+# Device-tensor API (torch for device memory and streams; the work is the C ABI's)
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_handle(stream=None) -> int:
+    torch = _torch()
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+class DenseMatcher:
+    """Device-resident matcher: images are CUDA uint8 tensors, outputs are CUDA
+    tensors, work is enqueued on the caller's current stream, and the workspace is
+    kept and reused across calls (grown when a larger batch needs it).
+
+    ``match`` / ``match_batch`` allocate only their output tensors (through torch's
+    caching allocator); ``match_into`` writes caller-provided outputs and allocates
+    nothing."""
+
+    def __init__(self, cfg: Optional[DeCfg] = None, device: int = 0):
+        torch = _torch()
+        self.cfg = cfg or Cfg()
+        self.device = torch.device("cuda", device)
+        self._ws = None
+
+    def workspace_bytes(self, shapes) -> int:
+        arr = (DePair * len(shapes))()
+        for i, s in enumerate(shapes):
+            W, H = s[0], s[1]
+            arr[i] = DePair(1, 1, W, H, s[2] if len(s) > 2 else 0, None, None, None, None)
+        n = C.c_size_t()
+        check(lib().de_dense_workspace_bytes(C.byref(self.cfg), arr, len(shapes), C.byref(n)))
+        return n.value
+
+    def _workspace(self, nbytes: int):
+        torch = _torch()
+        if self._ws is None or self._ws.numel() < nbytes:
+            self._ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def new_outputs(self, H: int, W: int, cand: bool = False) -> dict:
+        torch = _torch()
+        d = dict(disp=torch.empty((H, W), dtype=torch.float32, device=self.device),
+                 margin=torch.empty((H, W), dtype=torch.float32, device=self.device),
+                 conf=torch.empty((H, W), dtype=torch.uint8, device=self.device))
+        if cand:
+            d["cand"] = torch.empty((6, H, W), dtype=torch.float32, device=self.device)
+        return d
+
+    def match_into(self, items, stream=None) -> None:
+        """items: list of (L, R, dmax or 0, outputs dict).  Enqueues one batched launch
+        set on ``stream`` (default: current)."""
+        arr = (DePair * len(items))()
+        shapes = []
+        for i, (L, R, dmax, out) in enumerate(items):
+            if L.dtype != _torch().uint8 or L.device != self.device or not L.is_contiguous():
+                raise ValueError("images must be contiguous CUDA uint8 tensors on the device")
+            H, W = L.shape
+            shapes.append((W, H, dmax))
+            ptr = lambda k: out[k].data_ptr() if out.get(k) is not None else None  # noqa
+            arr[i] = DePair(L.data_ptr(), R.data_ptr(), W, H, dmax, ptr("disp"),
+                            ptr("margin"), ptr("conf"), ptr("cand"))
+        need = self.workspace_bytes(shapes)
+        ws = self._workspace(need)
+        check(lib().de_dense_dev(C.byref(self.cfg), arr, len(items), ws.data_ptr(), need,
+                                 _stream_handle(stream)))
+
+    def match(self, L, R, dmax: int = 0, cand: bool = False, stream=None) -> dict:
+        out = self.new_outputs(*L.shape, cand=cand)
+        self.match_into([(L, R, dmax, out)], stream)
+        return out
+
+    def match_batch(self, pairs, cand: bool = False, stream=None) -> list[dict]:
+        outs = [self.new_outputs(*p[0].shape, cand=cand) for p in pairs]
+        self.match_into([(p[0], p[1], p[2] if len(p) > 2 else 0, o)
+                         for p, o in zip(pairs, outs)], stream)
+        return outs
+
+
+# --------------------------------------------------------------------------------------
+# Stage entry points (device tensors), for stage-level parity and custom pipelines
+
+def census(L, R, cfg: Optional[DeCfg] = None, stream=None):
+    """Census words of both images (uint64 as int64 tensors) and the left image's
+    Q15 coefficient planes ax, ay (int16 tensors holding uint16 bit patterns)."""
+    torch = _torch()
+    cfg = cfg or Cfg()
+    H, W = L.shape
+    cl = torch.empty((H, W), dtype=torch.int64, device=L.device)
+    cr = torch.empty_like(cl)
+    ax = torch.empty((H, W), dtype=torch.int16, device=L.device)
+    ay = torch.empty_like(ax)
+    check(lib().de_census_dev(C.byref(cfg), L.data_ptr(), R.data_ptr(), W, H, cl.data_ptr(),
+                              cr.data_ptr(), ax.data_ptr(), ay.data_ptr(),
+                              _stream_handle(stream)))
+    return cl, cr, ax, ay
+
+
+def cost_top2(L, R, cfg: Optional[DeCfg] = None, stream=None):
+    """Candidates in the reference layout: cs f32 (H,W,2), cd i32 (H,W,2), cn i32 (H,W),
+    cnb i16 (H,W,2)."""
+    torch = _torch()
+    cfg = cfg or Cfg()
+    H, W = L.shape
+    D = cfg.dmax - cfg.dmin + 1
+    ws_n = lib().de_cost_workspace_bytes(W, H, D)
+    ws = torch.empty(ws_n, dtype=torch.uint8, device=L.device)
+    cs = torch.empty((H, W, 2), dtype=torch.float32, device=L.device)
+    cd = torch.empty((H, W, 2), dtype=torch.int32, device=L.device)
+    cn = torch.empty((H, W), dtype=torch.int32, device=L.device)
+    cnb = torch.empty((H, W, 2), dtype=torch.int16, device=L.device)
+    check(lib().de_cost_top2_dev(C.byref(cfg), L.data_ptr(), R.data_ptr(), W, H, cs.data_ptr(),
+                                 cd.data_ptr(), cn.data_ptr(), cnb.data_ptr(), ws.data_ptr(),
+                                 ws_n, _stream_handle(stream)))
+    return cs, cd, cn, cnb
+
+
+def solve(cs, cd, cn, cnb, cfg: Optional[DeCfg] = None, stream=None):
+    """Row solve over reference-layout candidates: disp, margin, lrc2 (H, W)."""
+    torch = _torch()
+    cfg = cfg or Cfg()
+    H, W = cn.shape
+    disp = torch.empty((H, W), dtype=torch.float32, device=cn.device)
+    margin = torch.empty_like(disp)
+    lrc2 = torch.empty_like(disp)
+    check(lib().de_solve_dev(C.byref(cfg), W, H, cs.data_ptr(), cd.data_ptr(), cn.data_ptr(),
+                             cnb.data_ptr() if cnb is not None else None, disp.data_ptr(),
+                             margin.data_ptr(), lrc2.data_ptr(), _stream_handle(stream)))
+    return disp, margin, lrc2
+
+
+def confidence(s1: float, s2: float, lam: float = -0.1, lrc: float = 0.0,
+               lrc_tol: float = 1.0) -> float:
+    """confidence() of core/include/doubleeye/dense_solve.hpp:158 (host)."""
+    return lib().de_confidence(s1, s2, lam, lrc, lrc_tol)

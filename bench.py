@@ -1,0 +1,361 @@
+"""Benchmark: dense MASDA stereo at 848x480, D=128, 8 BP iterations (pairs/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--pairs-per-step B]
+
+A step is one batched pass of the whole hot path (census -> cost -> 4-pass filter
+-> top-2 -> row solve) over B distinct seeded 848x480 pairs already resident in HBM.
+``value`` is whole-job pairs/s (all ranks).  Multi-GPU runs are independent replicas
+(pairs need no exchange): each rank matches its own B pairs per step; timing is the
+max over ranks of CUDA-event time.  ``e2e`` is the same metric through the public
+host API (host arrays in, host arrays out, copies inside the timed region).
+
+``--impl reference`` times the reference's own CPU implementation of the path
+(oracle/_ref, the reference compiled from its sources; else this repository's C
+restatement) on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+W, H, D, ITERS = 848, 480, 128, 8
+METRIC = "stereo pairs/s, dense MASDA 848x480 D=128 8 BP iters"
+
+
+def disp_evals(n_pairs: int) -> float:
+    return float(n_pairs) * W * H * D
+
+
+# Algorithmic bytes per pair and per stage ("Roofline"): compulsory
+# traffic of each kernel if every operand is touched once.
+WH = W * H
+E = WH * D
+ALG_BYTES = {
+    "census": 2 * WH + 16 * WH + 4 * WH,        # read L,R; write census words, ax, ay
+    "rows": 16 * WH + 2 * WH + 2 * E,           # read census words + ax; write volume
+    "cols": 2 * E + 2 * WH + 12 * WH,           # read volume + ay; write candidates
+    "solve": 12 * WH + 9 * WH,                  # read candidates; write disp, margin, conf
+    "pipeline": 2 * WH + 4 * E + 24 * WH + 8 * WH,
+}
+STAGES = ["census", "rows", "cols", "solve"]
+
+
+def load_peaks() -> dict:
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": d["hbm_gbs"], "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+def ncu_traffic() -> dict:
+    p = os.path.join(REPO, "profiles", "ncu_dram_bytes.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_pairs(n: int, seed0: int):
+    from doubleeye_b200 import synth
+    return [synth.slanted_planes(W, H, D - 1, seed=seed0 + i, tag="bench") for i in range(n)]
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline_sample(budget_s: float = 12.0, max_pairs: int = 24) -> dict:
+    """The reference's CPU path on this host's cores, bounded sample."""
+    from oracle import oracle as O
+    nthreads = os.cpu_count() or 1
+    pairs = make_pairs(3, 900)
+    cfg = O.default_cfg(dmax=D, iters=ITERS)
+    if O.Reference.available():
+        ref = O.Reference()
+        run = lambda p: ref.dense(cfg, p.left, p.right, nthreads=nthreads, want_cand=False)  # noqa
+        kind, cores = "reference", nthreads
+    else:
+        orc = O.Oracle()
+        run = lambda p: orc.dense(cfg, p.left, p.right, want_cand=False)  # noqa
+        kind, cores = "port", 1
+    run(pairs[0])                                  # warm caches
+    n, t0 = 0, time.perf_counter()
+    while n < max_pairs and time.perf_counter() - t0 < budget_s:
+        run(pairs[n % len(pairs)])
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
+            "sample": f"{n} pairs 848x480 D=128 iters 8 in {dt:.1f}s, "
+                      f"{'de_dense run_dense' if kind == 'reference' else 'oracle port'}"
+                      f" at {cores} thread(s)"}
+
+
+def run_reference(args) -> None:
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    nthreads = os.cpu_count() or 1
+    cfg = O.default_cfg(dmax=D, iters=ITERS)
+    pairs = make_pairs(args.ref_sample, 0)
+    if O.Reference.available():
+        ref = O.Reference()
+        run = lambda p: ref.dense(cfg, p.left, p.right, nthreads=nthreads, want_cand=False)  # noqa
+        kind, cores, what = "reference", nthreads, "reference run_dense (core/tools/de_dense.cpp)"
+    else:
+        orc = O.Oracle()
+        run = lambda p: orc.dense(cfg, p.left, p.right, want_cand=False)  # noqa
+        kind, cores, what = "port", 1, "oracle C restatement"
+    for _ in range(args.warmup):
+        for p in pairs:
+            run(p)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for p in pairs:
+            run(p)
+    dt = time.perf_counter() - t0
+    n = args.steps * len(pairs)
+    v = n / dt
+    out = {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "i16/f32",
+           "data": "synthetic (seeded slanted planes)", "impl": "reference",
+           "config": {"workload": "dense 848x480 D=128 iters=8", "W": W, "H": H, "D": D,
+                      "iters": ITERS, "pairs_per_step": len(pairs), "parallelism": "cpu"},
+           "g_disp_evals_per_s": disp_evals(n) / dt / 1e9,
+           "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": kind,
+                            "sample": f"{len(pairs)} pairs per step, {what}, "
+                                      f"{cores} thread(s)"},
+           "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args) -> None:
+    import torch
+    import doubleeye_b200 as de
+    from doubleeye_b200 import build
+    from doubleeye_b200._lib import check, lib
+    build.build()
+    ws, rank, local = dist_setup()
+    B, K, Wm = args.pairs_per_step, args.steps, args.warmup
+    pairs = make_pairs(B, 1000 * rank)
+    cfg = de.Cfg(dmax=D, iters=ITERS)
+    m = de.DenseMatcher(cfg, device=local)
+    Ls = [torch.from_numpy(p.left).cuda() for p in pairs]
+    Rs = [torch.from_numpy(p.right).cuda() for p in pairs]
+    outs = [m.new_outputs(H, W) for _ in pairs]
+    items = [(L, R, 0, o) for L, R, o in zip(Ls, Rs, outs)]
+    stream = torch.cuda.current_stream()
+
+    # --- device-timed batched throughput (the headline value) -----------------------
+    for _ in range(Wm):
+        m.match_into(items)
+    torch.cuda.synchronize()
+    barrier(ws)
+    lib().de_stage_timing(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier(ws)
+        e0.record(stream)
+        for _ in range(K):
+            m.match_into(items)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    lib().de_stage_timing(0)
+    barrier(ws)
+    ms_local = e0.elapsed_time(e1)
+    stage = (C.c_float * 4)()
+    nl = C.c_int()
+    check(lib().de_stage_times(stage, 4, C.byref(nl)))
+    ms = max_over_ranks(ms_local, ws)
+    total_pairs = ws * B * K
+    value = total_pairs / (ms / 1e3)
+
+    # --- plain single-pair path, same device timing -------------------------------
+    one = [items[0]]
+    for _ in range(Wm):
+        m.match_into(one)
+    torch.cuda.synchronize()
+    barrier(ws)
+    e0.record(stream)
+    for _ in range(K):
+        m.match_into(one)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain = ws * K / (max_over_ranks(e0.elapsed_time(e1), ws) / 1e3)
+
+    # --- end to end through the public host API -----------------------------------
+    host = [(p.left, p.right) for p in pairs]
+    for _ in range(max(1, Wm // 2)):
+        res = de.run_dense_batch(host, cfg, device=local)
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(K):
+        res = de.run_dense_batch(host, cfg, device=local)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
+    filled = float(np.mean([np.isfinite(r.disp).mean() for r in res]))
+
+    # --- roofline of the dominant kernel ------------------------------------------
+    per_launch = {s: stage[i] / max(1, nl.value) for i, s in enumerate(STAGES)}
+    dom = max(STAGES, key=lambda s: per_launch[s])
+    peaks = load_peaks()
+    alg = ALG_BYTES[dom] * B                      # one launch processes B pairs
+    achieved = alg / (per_launch[dom] / 1e3) / 1e9
+    traffic = ncu_traffic().get(dom)
+    roof = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved,
+            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+            "peak_src": peaks["src"],
+            "traffic": traffic * B if traffic is not None else None,
+            "alg_bytes_per_launch": alg,
+            "pipeline_frac": ALG_BYTES["pipeline"] * B * K / (ms / 1e3) / 1e9
+            / peaks["hbm_gbs"] / ws}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": K,
+               "warmup": Wm, "ms_per_step": ms / K, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "i16/f32",
+               "data": "synthetic (seeded slanted planes, 12 planes, grad<=0.15, "
+                       "occlusion refill, +-5% gain/offset)",
+               "config": {"workload": "dense 848x480 D=128 iters=8", "W": W, "H": H, "D": D,
+                          "iters": ITERS, "pairs_per_step": B,
+                          "parallelism": f"replicas x{ws}" if ws > 1 else "single",
+                          "l2": f"working set > L2 ({B} pairs x "
+                                f"{m.workspace_bytes([(W, H, 0)]) / 1e6:.0f} MB)"},
+               "g_disp_evals_per_s": disp_evals(total_pairs) / (ms / 1e3) / 1e9,
+               "plain_pairs_per_s": plain, "batch_over_plain": value / plain,
+               "stage_ms_per_launch": per_launch, "filled": filled,
+               "roofline": roof,
+               "clocks": clk.summary(),
+               "e2e": {"value": ws * B * K / e2e_s, "unit": "pairs/s",
+                       "h2d_bytes_per_step": B * 2 * WH,
+                       "d2h_bytes_per_step": B * 9 * WH},
+               "gpu_launches": 4 * K * ((B + 63) // 64)}
+        if ws == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline_sample()
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--pairs-per-step", type=int, default=16)
+    ap.add_argument("--ref-sample", type=int, default=2, help="pairs per reference step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

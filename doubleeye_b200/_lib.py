@@ -93,6 +93,10 @@ SIGNATURES = {
     "de_solve_dev": (C.c_int, [C.POINTER(DeCfg), C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp,
                                vp]),
     "de_confidence": (C.c_float, [C.c_float] * 5),
+    "de_stage_timing": (C.c_int, [C.c_int]),
+    "de_set_param": (C.c_int, [C.c_char_p, C.c_int]),
+    "de_get_param": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
+    "de_stage_times": (C.c_int, [C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
     "de_ctx_create": (C.c_int, [C.POINTER(DeCfg), C.c_int, C.POINTER(vp)]),
     "de_ctx_destroy": (C.c_int, [vp]),
     "de_ctx_set_cfg": (C.c_int, [vp, C.POINTER(DeCfg)]),
@@ -128,6 +132,16 @@ def lib() -> C.CDLL:
 def check(rc: int) -> None:
     if rc != DE_OK:
         raise DeError(rc, lib().de_last_error().decode(errors="replace"))
+
+
+def set_param(name: str, value: int) -> None:
+    check(lib().de_set_param(name.encode(), int(value)))
+
+
+def get_param(name: str) -> int:
+    v = C.c_int()
+    check(lib().de_get_param(name.encode(), C.byref(v)))
+    return v.value
 
 
 def exported_symbols() -> list[str]:

@@ -185,16 +185,45 @@ void fill_batch(const de_cfg& c, const de_pair* pairs, int first, int n, uint8_t
   }
 }
 
+// Optional stage timing: CUDA events recorded on the launching stream between the
+// stages of every de_dense_dev launch set while enabled (the counterpart of the
+// reference's event breakdown, core/tools/de_dense_cuda.cu:552-604).
+struct StageTimer {
+  std::mutex mu;
+  bool on = false;
+  std::vector<cudaEvent_t> ev;   // groups of 5: before census, rows, cols, solve, after
+} g_timer;
+
+void timer_mark(cudaStream_t s, std::vector<cudaEvent_t>* group) {
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) == cudaSuccess) {
+    cudaEventRecord(e, s);
+    group->push_back(e);
+  }
+}
+
 int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
   de::DevCfg dc;
   de::make_dev_cfg(c, &dc);
   if (c.lrc)
     for (int i = 0; i < b.n; ++i)
       DE_CUDA(cudaMemsetAsync(b.p[i].rkey, 0, size_t(b.p[i].W) * b.p[i].H * 4, s));
+  std::vector<cudaEvent_t> grp;
+  const bool timed = g_timer.on;
+  if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_census(dc, b, s));
+  if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_rows(dc, b, s));
+  if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_cols(dc, b, s));
+  if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_solve(dc, b, false, s));
+  if (timed) {
+    timer_mark(s, &grp);
+    std::lock_guard<std::mutex> lk(g_timer.mu);
+    if (grp.size() == 5) g_timer.ev.insert(g_timer.ev.end(), grp.begin(), grp.end());
+    else for (cudaEvent_t e : grp) cudaEventDestroy(e);
+  }
   return DE_OK;
 }
 
@@ -371,6 +400,48 @@ int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const int* cd
   b.solve_prefix[1] = H;
   DE_CUDA(de::launch_solve(dc, b, true, static_cast<cudaStream_t>(stream)));
   return DE_OK;
+}
+
+int de_stage_timing(int enable) {
+  std::lock_guard<std::mutex> lk(g_timer.mu);
+  g_timer.on = enable != 0;
+  return DE_OK;
+}
+
+int de_stage_times(float* ms, int n, int* launches) {
+  std::lock_guard<std::mutex> lk(g_timer.mu);
+  for (int i = 0; i < n; ++i) ms[i] = 0.f;
+  int groups = 0;
+  cudaError_t err = cudaSuccess;
+  for (size_t g = 0; g + 5 <= g_timer.ev.size(); g += 5, ++groups)
+    for (int k = 0; k < 4 && k < n; ++k) {
+      float t = 0.f;
+      cudaError_t e = cudaEventSynchronize(g_timer.ev[g + k + 1]);
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&t, g_timer.ev[g + k], g_timer.ev[g + k + 1]);
+      if (e != cudaSuccess) err = e;
+      ms[k] += t;
+    }
+  for (cudaEvent_t e : g_timer.ev) cudaEventDestroy(e);
+  g_timer.ev.clear();
+  if (launches) *launches = groups;
+  if (err != cudaSuccess) return cuda_fail(err, "stage timing events");
+  return DE_OK;
+}
+
+int de_set_param(const char* name, int value) {
+  if (!name) return fail(DE_ERR_ARG, "name is NULL");
+  if (!std::strcmp(name, "rows_ctas_per_sm")) { de::set_rows_ctas_per_sm(value); return DE_OK; }
+  if (!std::strcmp(name, "cols_kt")) { de::set_cols_kt(value); return DE_OK; }
+  if (!std::strcmp(name, "rows_table_copies")) { de::set_rows_table_copies(value); return DE_OK; }
+  return fail(DE_ERR_ARG, "unknown parameter %s", name);
+}
+
+int de_get_param(const char* name, int* value) {
+  if (!name || !value) return fail(DE_ERR_ARG, "NULL argument");
+  if (!std::strcmp(name, "rows_ctas_per_sm")) { *value = de::get_rows_ctas_per_sm(); return DE_OK; }
+  if (!std::strcmp(name, "cols_kt")) { *value = de::get_cols_kt(); return DE_OK; }
+  if (!std::strcmp(name, "rows_table_copies")) { *value = de::get_rows_table_copies(); return DE_OK; }
+  return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 
 // confidence(), core/include/doubleeye/dense_solve.hpp:158-166.

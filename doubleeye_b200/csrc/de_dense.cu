@@ -29,6 +29,7 @@
 // capturable).  Compiled with --fmad=false: the solve's float arithmetic must not
 // be contracted, to match the reference's x86-64 single-precision results.
 
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -127,121 +128,188 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
 // at its first lane's start.  Values left of a plane's valid window never reach a
 // valid output (the vertical passes stay within a column and the top-2 masks
 // k > x - hw - dmin), so they are not computed exactly and not needed.
-template <bool PACKED, int TS>
-__device__ __forceinline__ int32_t graded(uint64_t lw, uint64_t rw, const int16_t* stab,
+// Score table: (h, m) -> Q14 score, h = Hamming distance, m = |L - R| clamped to
+// TS-1 (exact: the AD score saturates at ad_trunc < TS).  With TS = 16 the table is
+// stored as int32 in 8 interleaved copies (lane l reads copy l & 7), which spreads
+// the warp's data-dependent lookups over the shared-memory banks.
+template <int TS, int CP>
+struct ScoreTable {
+  __host__ __device__ static constexpr size_t bytes() {
+    return CP == 2 ? size_t(96) * 4 : size_t(66) * TS * (TS == 16 ? 4 * CP : 2);
+  }
+};
+
+template <bool PACKED, int TS, int CP>
+__device__ __forceinline__ int32_t graded(uint64_t lw, uint64_t rw, const void* tab,
                                           const uint8_t* sLp, const uint8_t* sRp, int xl,
                                           int xr) {
   int h, ad;
   if (PACKED) {
     const uint32_t lo = uint32_t(lw) ^ uint32_t(rw);
-    const uint32_t hi = (uint32_t(lw >> 32) ^ uint32_t(rw >> 32));
+    const uint32_t hi = uint32_t(lw >> 32) ^ uint32_t(rw >> 32);
     h = __popc(lo) + __popc(hi & 0x00FFFFFFu);
     ad = abs(int(uint32_t(lw >> 56)) - int(uint32_t(rw >> 56)));
   } else {
     h = __popcll(lw ^ rw);
     ad = abs(int(sLp[xl]) - int(sRp[xr]));
   }
-  if (TS == 16) ad = min(ad, 15);
-  return stab[h * TS + ad];
+  if (TS == 16 && CP == 2) {           // v = (C1[h] + A1[m]) >> 10, two small tables
+    ad = min(ad, 15);
+    const int32_t* t = static_cast<const int32_t*>(tab);
+    return (t[h] + t[66 + ad]) >> 10;
+  }
+  if (TS == 16) {
+    ad = min(ad, 15);
+    return static_cast<const int32_t*>(tab)[(h * 16 + ad) * CP];
+  }
+  return static_cast<const int16_t*>(tab)[h * TS + ad];
 }
 
-template <bool PACKED, int TS>
+template <bool PACKED, int TS, int CP>
 __global__ void __launch_bounds__(128) k_rows(DevCfg cfg, Batch b) {
   extern __shared__ __align__(16) uint8_t smem[];
-  const int item = blockIdx.x;
-  const int pi = find_pair(b.rows_prefix, b.n, item);
-  const DevPair& P = b.p[pi];
-  const int W = P.W, Dpad = P.Dpad;
-  const int y = cfg.hh + (item - b.rows_prefix[pi]);
+  // shared layout: table | sL (+1 word pad) | sR | sax (+pad) | sLp | sRp
+  int maxW = 0;
+  for (int i = 0; i < b.n; ++i) maxW = max(maxW, b.p[i].W);
+  uint8_t* tabp = smem;
+  uint64_t* sLraw = reinterpret_cast<uint64_t*>(tabp + ScoreTable<TS, CP>::bytes());
+  uint64_t* sR = sLraw + ((maxW + 2) & ~1);
+  uint16_t* saxraw = reinterpret_cast<uint16_t*>(sR + ((maxW + 1) & ~1));
+  uint8_t* sLp = reinterpret_cast<uint8_t*>(saxraw + ((maxW + 9) & ~7));
+  uint8_t* sRp = sLp + maxW;
+  // table, once per CTA
+  if (TS == 16 && CP == 2) {
+    int32_t* t32 = reinterpret_cast<int32_t*>(tabp);
+    for (int i = threadIdx.x; i < 96; i += blockDim.x)
+      t32[i] = i < 66 ? int32_t(cfg.tbl[i]) * (1024 - cfg.wq)
+                      : (i < 82 ? int32_t(cfg.adt[i - 66]) * cfg.wq : 0);
+  } else if (TS == 16) {
+    int32_t* t32 = reinterpret_cast<int32_t*>(tabp);
+    for (int i = threadIdx.x; i < 66 * 16 * CP; i += blockDim.x) {
+      const int e = i / CP, h = e >> 4, m = e & 15;
+      t32[i] = (int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10;
+    }
+  } else {
+    int16_t* t16 = reinterpret_cast<int16_t*>(tabp);
+    for (int i = threadIdx.x; i < 66 * TS; i += blockDim.x) {
+      const int h = i / TS, m = i % TS;
+      t16[i] = int16_t((int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10);
+    }
+  }
+  const void* tab = (TS == 16 && CP != 2) ? static_cast<const void*>(reinterpret_cast<const int32_t*>(tabp) + (threadIdx.x % CP))
+                               : static_cast<const void*>(tabp);
   const int hw = cfg.hw, dmin = cfg.dmin;
-  uint64_t* sL = reinterpret_cast<uint64_t*>(smem);
-  uint64_t* sR = sL + W;
-  uint16_t* sax = reinterpret_cast<uint16_t*>(sR + W);
-  int16_t* stab = reinterpret_cast<int16_t*>(sax + ((W + 7) & ~7));
-  uint8_t* sLp = reinterpret_cast<uint8_t*>(stab + 66 * TS);
-  uint8_t* sRp = sLp + W;
-  const size_t row = size_t(y) * W;
-  for (int i = threadIdx.x; i < W; i += blockDim.x) {
-    sL[i] = P.cwL[row + i];
-    sR[i] = P.cwR[row + i];
-    sax[i] = P.ax[row + i];
-    if (!PACKED) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
-  }
-  for (int i = threadIdx.x; i < 66 * TS; i += blockDim.x) {
-    const int h = i / TS, m = i % TS;
-    stab[i] = int16_t((int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10);
-  }
-  __syncthreads();
   const int t = threadIdx.x;
-  if (2 * t >= Dpad) return;
-  const int d0 = dmin + 2 * t;
-  const int xw = hw + dmin + 2 * (t & ~31);          // first lane's start in this warp
-  const int xend = W - hw;                            // scores are 0 from here on
-  uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * Dpad) + t;
-  const size_t xs = size_t(Dpad) >> 1;                // x stride in 32-bit words
-  int32_t f0 = 0, f1 = 0;
-  // previous step's right word = chain k1's word at the first step
-  uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;
-  int x = xw;
-  // ramp: lanes may not have reached their own valid start yet
-  const int xramp = min(xend, xw + 64);
-  for (; x < xramp; ++x) {
-    const int32_t a = sax[x];
-    const uint64_t lw = sL[x];
-    int32_t v0 = 0, v1 = 0;
-    uint64_t rw = 0;
-    if (x - d0 >= hw) {
-      rw = sR[x - d0];
-      v0 = graded<PACKED, TS>(lw, rw, stab, sLp, sRp, x, x - d0);
+  // sL / sax are offset by (dmin & 1) elements so that x with (x - dmin) even sits on a
+  // 16-byte (sL) / 4-byte (sax) boundary, like sR[x - d] for every lane.
+  uint64_t* sL = sLraw + (dmin & 1);
+  uint16_t* sax = saxraw + (dmin & 1);
+  const int total = b.rows_prefix[b.n];
+  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+    const int pi = find_pair(b.rows_prefix, b.n, item);
+    const DevPair& P = b.p[pi];
+    const int W = P.W, Dpad = P.Dpad;
+    const int y = cfg.hh + (item - b.rows_prefix[pi]);
+    const size_t row = size_t(y) * W;
+    __syncthreads();                                   // previous row's readers are done
+    for (int i = threadIdx.x; i < W; i += blockDim.x) {
+      sL[i] = P.cwL[row + i];
+      sR[i] = P.cwR[row + i];
+      sax[i] = P.ax[row + i];
+      if (!PACKED) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
     }
-    if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS>(lw, rprev, stab, sLp, sRp, x, x - d0 - 1);
-    rprev = rw;
-    f0 = rf_step(v0, f0, a);
-    f1 = rf_step(v1, f1, a);
-    out[x * xs] = pack2(f0, f1);
-  }
-  // main: every chain in the warp is inside its window
-#pragma unroll 4
-  for (; x < xend; ++x) {
-    const int32_t a = sax[x];
-    const uint64_t lw = sL[x];
-    const uint64_t rw = sR[x - d0];
-    const int32_t v0 = graded<PACKED, TS>(lw, rw, stab, sLp, sRp, x, x - d0);
-    const int32_t v1 = graded<PACKED, TS>(lw, rprev, stab, sLp, sRp, x, x - d0 - 1);
-    rprev = rw;
-    f0 = rf_step(v0, f0, a);
-    f1 = rf_step(v1, f1, a);
-    out[x * xs] = pack2(f0, f1);
-  }
-  // tail: right border, score 0
-  for (; x < W; ++x) {
-    const int32_t a = sax[x];
-    f0 = rf_step(0, f0, a);
-    f1 = rf_step(0, f1, a);
-    out[x * xs] = pack2(f0, f1);
-  }
-  // backward: seed with the forward value at W-1 (already stored), coefficient at x+1
-  int32_t g0 = f0, g1 = f1;
-  const int xlo = xw;
-  x = W - 2;
-  constexpr int PF = 8;
-  uint32_t ring[PF];
-#pragma unroll
-  for (int j = 0; j < PF; ++j) ring[j] = (x - j >= xlo) ? out[(x - j) * xs] : 0u;
-  while (x >= xlo) {
-#pragma unroll
-    for (int j = 0; j < PF; ++j) {
-      const int xx = x - j;
-      if (xx >= xlo) {
-        const uint32_t c = ring[j];
-        const int32_t a = sax[xx + 1];
-        g0 = rf_step(lo16(c), g0, a);
-        g1 = rf_step(hi16(c), g1, a);
-        ring[j] = (xx - PF >= xlo) ? out[(xx - PF) * xs] : 0u;
-        out[xx * xs] = pack2(g0, g1);
+    __syncthreads();
+    if (2 * t >= Dpad) continue;
+    const int d0 = dmin + 2 * t;
+    const int xw = hw + dmin + 2 * (t & ~31);          // first lane's start in this warp
+    const int xend = W - hw;                            // scores are 0 from here on
+    uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * Dpad) + t;
+    const size_t xs = size_t(Dpad) >> 1;                // x stride in 32-bit words
+    int32_t f0 = 0, f1 = 0;
+    uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;   // chain k1's word
+    int x = xw;
+    // ramp: lanes may not have reached their own valid start yet; ends on an x with
+    // (x - dmin) even so the paired loop below is aligned
+    int xramp = min(xend, xw + 64);
+    xramp += (xramp - dmin) & 1;
+    xramp = min(xramp, xend);
+    for (; x < xramp; ++x) {
+      const int32_t a = sax[x];
+      const uint64_t lw = sL[x];
+      int32_t v0 = 0, v1 = 0;
+      uint64_t rw = 0;
+      if (x - d0 >= hw) {
+        rw = sR[x - d0];
+        v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
       }
+      if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
+      rprev = rw;
+      f0 = rf_step(v0, f0, a);
+      f1 = rf_step(v1, f1, a);
+      out[x * xs] = pack2(f0, f1);
     }
-    x -= PF;
+    // main: two x per iteration, every chain in the warp inside its window
+#pragma unroll 2
+    for (; x + 1 < xend; x += 2) {
+      const uint32_t a2 = *reinterpret_cast<const uint32_t*>(sax + x);
+      const ulonglong2 l2 = *reinterpret_cast<const ulonglong2*>(sL + x);
+      const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(sR + (x - d0));
+      const int32_t a0 = int32_t(a2 & 0xFFFFu), a1 = int32_t(a2 >> 16);
+      // x:   chain0 <- r2.x (x - d0), chain1 <- rprev (x - d0 - 1)
+      // x+1: chain0 <- r2.y,          chain1 <- r2.x
+      const int32_t v00 = graded<PACKED, TS, CP>(l2.x, r2.x, tab, sLp, sRp, x, x - d0);
+      const int32_t v01 = graded<PACKED, TS, CP>(l2.x, rprev, tab, sLp, sRp, x, x - d0 - 1);
+      const int32_t v10 = graded<PACKED, TS, CP>(l2.y, r2.y, tab, sLp, sRp, x + 1, x + 1 - d0);
+      const int32_t v11 = graded<PACKED, TS, CP>(l2.y, r2.x, tab, sLp, sRp, x + 1, x - d0);
+      rprev = r2.y;
+      f0 = rf_step(v00, f0, a0);
+      f1 = rf_step(v01, f1, a0);
+      out[x * xs] = pack2(f0, f1);
+      f0 = rf_step(v10, f0, a1);
+      f1 = rf_step(v11, f1, a1);
+      out[(x + 1) * xs] = pack2(f0, f1);
+    }
+    for (; x < xend; ++x) {                          // at most one leftover step
+      const int32_t a = sax[x];
+      const uint64_t lw = sL[x];
+      const uint64_t rw = sR[x - d0];
+      const int32_t v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
+      const int32_t v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
+      rprev = rw;
+      f0 = rf_step(v0, f0, a);
+      f1 = rf_step(v1, f1, a);
+      out[x * xs] = pack2(f0, f1);
+    }
+    for (; x < W; ++x) {                             // right border, score 0
+      const int32_t a = sax[x];
+      f0 = rf_step(0, f0, a);
+      f1 = rf_step(0, f1, a);
+      out[x * xs] = pack2(f0, f1);
+    }
+    // backward: seed with the forward value at W-1 (already stored), coefficient at
+    // x+1; the forward results come back through L2, prefetched PF columns ahead
+    int32_t g0 = f0, g1 = f1;
+    const int xlo = xw;
+    x = W - 2;
+    constexpr int PF = 32;
+    uint32_t ring[PF];
+#pragma unroll
+    for (int j = 0; j < PF; ++j) ring[j] = (x - j >= xlo) ? out[(x - j) * xs] : 0u;
+    while (x >= xlo) {
+#pragma unroll
+      for (int j = 0; j < PF; ++j) {
+        const int xx = x - j;
+        if (xx >= xlo) {
+          const uint32_t c = ring[j];
+          const int32_t a = sax[xx + 1];
+          g0 = rf_step(lo16(c), g0, a);
+          g1 = rf_step(hi16(c), g1, a);
+          ring[j] = (xx - PF >= xlo) ? out[(xx - PF) * xs] : 0u;
+          out[xx * xs] = pack2(g0, g1);
+        }
+      }
+      x -= PF;
+    }
   }
 }
 
@@ -249,127 +317,149 @@ __global__ void __launch_bounds__(128) k_rows(DevCfg cfg, Batch b) {
 // k_cols: vertical forward (in place), vertical backward + top-2 + neighbours.
 // Vertical passes: core/tools/de_dense.cpp:490-507.  Top-2 semantics: :1276-1292
 // (ascending k, strictly greater, ties keep the smaller k), sub-pixel neighbour
-// capture :1276-1285.  The packed key ((v + 32768) << 8 | (255 - k)) makes the
-// reduction order-independent, so a shuffle tree reproduces the sequential scan.
-template <int G>
+// capture :1276-1285.
+//
+// A column is a group of TPC = Dpad/KT lanes (padded to TPCP, a power of two);
+// lane s of the group owns disparities [s*KT, s*KT + KT) as int16 pairs, so one row
+// of one column is 2*Dpad contiguous bytes read with 128-bit loads, and adjacent
+// columns are adjacent in memory.  The top-2 key (v + 32768) << 8 | (255 - k) is
+// unique per k, so the strictly-greater insertion is three unsigned min/max, the
+// merge across lanes is four, and any merge order gives the sequential scan's
+// answer.  The winner's neighbour costs are read back from a per-warp row buffer.
+__device__ __forceinline__ int32_t sx16(uint32_t v) {     // sign-extended low half
+  return int32_t(int16_t(uint16_t(v & 0xFFFFu)));
+}
+__device__ __forceinline__ int32_t hx16(uint32_t v) { return int32_t(v) >> 16; }
+__device__ __forceinline__ uint32_t pk16(int32_t lo, int32_t hi) {
+  return __byte_perm(uint32_t(lo), uint32_t(hi), 0x5410);
+}
+
+template <int KT, int TPCP>
 __global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= b.cols_prefix[b.n]) return;
-  const int pi = find_pair(b.cols_prefix, b.n, warp);
+  static_assert(KT % 8 == 0 && TPCP >= 1 && TPCP <= 32, "shape");
+  constexpr int NV = KT / 8;                         // 128-bit vectors per row
+  constexpr int PF = 4;                              // rows prefetched ahead
+  __shared__ __align__(16) int16_t sbuf[256 / 32][32 * KT];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int group = (blockIdx.x * blockDim.x + threadIdx.x) / TPCP;
+  const int sub = lane % TPCP, gbase = lane - sub;
+  const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
+  if (group >= b.cols_prefix[b.n]) return;           // whole groups leave together
+  const int pi = find_pair(b.cols_prefix, b.n, group);
   const DevPair& P = b.p[pi];
   const int W = P.W, H = P.H, D = P.D, Dpad = P.Dpad;
   const int hw = cfg.hw, hh = cfg.hh, dmin = cfg.dmin;
-  const int x = hw + dmin + (warp - b.cols_prefix[pi]);
+  const int x = hw + dmin + (group - b.cols_prefix[pi]);
   const int kmax = min(D - 1, x - hw - dmin);
-  const int Gp = Dpad >> 6;                          // this pair's groups (<= G)
-  uint32_t* col = reinterpret_cast<uint32_t*>(P.vol + size_t(x) * Dpad) + lane;
-  const size_t rs = size_t(W) * Dpad / 2;           // row stride, 32-bit words
+  const int k0 = sub * KT;
+  const bool live = k0 < Dpad;                       // lanes past this pair's Dpad idle
+  const int nvalid = max(0, min(KT, kmax - k0 + 1));
+  uint4* col = reinterpret_cast<uint4*>(P.vol + size_t(x) * Dpad + (live ? k0 : 0));
+  const size_t rs = size_t(W) * Dpad / 8;            // row stride in uint4
   const uint16_t* ay = P.ay + x;
-  int32_t p0[G], p1[G];
+  const int yin = H - hh;                            // rows >= yin have zero input
+  int32_t st[KT];
 #pragma unroll
-  for (int g = 0; g < G; ++g) { p0[g] = 0; p1[g] = 0; }
-  // forward: rows < hh are zero, rows >= H-hh have zero input
-  const int yin = H - hh;
-  constexpr int PF = 4;
-  uint32_t ring[PF][G];
+  for (int s = 0; s < KT; ++s) st[s] = 0;
+  uint4 ring[PF][NV];
+  auto load_row = [&](int y, uint4* dst) {
 #pragma unroll
-  for (int j = 0; j < PF; ++j)
+    for (int v = 0; v < NV; ++v)
+      dst[v] = (live && y >= hh && y < yin) ? col[size_t(y) * rs + v] : make_uint4(0, 0, 0, 0);
+  };
+  auto step = [&](const uint4* src, int32_t a) {
 #pragma unroll
-    for (int g = 0; g < G; ++g)
-      ring[j][g] = (g < Gp && hh + j < yin) ? col[size_t(hh + j) * rs + g * 32] : 0u;
+    for (int v = 0; v < NV; ++v) {
+      const uint32_t w[4] = {src[v].x, src[v].y, src[v].z, src[v].w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        st[8 * v + 2 * j] = rf_step(sx16(w[j]), st[8 * v + 2 * j], a);
+        st[8 * v + 2 * j + 1] = rf_step(hx16(w[j]), st[8 * v + 2 * j + 1], a);
+      }
+    }
+  };
+  // ---- forward, rows hh..H-1 (rows < hh are zero and leave the carry at 0) ----
+#pragma unroll
+  for (int j = 0; j < PF; ++j) load_row(hh + j, ring[j]);
   for (int y0 = hh; y0 < H; y0 += PF) {
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
       const int y = y0 + j;
       if (y < H) {
         const int32_t a = ay[size_t(y) * W];
+        step(ring[j], a);
+        load_row(y + PF, ring[j]);
+        if (live) {
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-          if (g >= Gp) break;
-          const uint32_t c = ring[j][g];
-          ring[j][g] = (y + PF < yin) ? col[size_t(y + PF) * rs + g * 32] : 0u;
-          p0[g] = rf_step(lo16(c), p0[g], a);
-          p1[g] = rf_step(hi16(c), p1[g], a);
-          col[size_t(y) * rs + g * 32] = pack2(p0[g], p1[g]);
+          for (int v = 0; v < NV; ++v)
+            col[size_t(y) * rs + v] =
+                make_uint4(pk16(st[8 * v], st[8 * v + 1]), pk16(st[8 * v + 2], st[8 * v + 3]),
+                           pk16(st[8 * v + 4], st[8 * v + 5]), pk16(st[8 * v + 6], st[8 * v + 7]));
         }
       }
     }
   }
-  // backward from H-1 (its value is the forward value), coefficient at y+1
-  uint32_t* key0 = P.key0 + x;
-  uint32_t* key1 = P.key1 + x;
-  uint32_t* nbp = P.nb + x;
+  // ---- backward from H-1 (its value is the forward one), coefficient at y+1 ----
+  auto load_fwd = [&](int y, uint4* dst) {            // rows written by the forward pass
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+      dst[v] = (live && y >= hh) ? col[size_t(y) * rs + v] : make_uint4(0, 0, 0, 0);
+  };
+#pragma unroll
+  for (int j = 0; j < PF; ++j) load_fwd(H - 2 - j, ring[j]);
   uint32_t* rkey = P.rkey;
-#pragma unroll
-  for (int j = 0; j < PF; ++j)
-#pragma unroll
-    for (int g = 0; g < G; ++g)
-      ring[j][g] = (g < Gp && H - 2 - j >= hh) ? col[size_t(H - 2 - j) * rs + g * 32] : 0u;
+  int16_t* rowbuf = &sbuf[wib][gbase * KT];
   for (int y0 = H - 2; y0 >= hh; y0 -= PF) {
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
       const int y = y0 - j;
       if (y >= hh) {
         const int32_t a = ay[size_t(y + 1) * W];
-        uint32_t pk0 = 0, pk1 = 0;
+        step(ring[j], a);
+        load_fwd(y - PF, ring[j]);
+        if (y < yin) {
+          uint32_t pk0 = 0, pk1 = 0;
 #pragma unroll
-        for (int g = 0; g < G; ++g) {
-          if (g >= Gp) break;
-          const uint32_t c = ring[j][g];
-          ring[j][g] = (y - PF >= hh) ? col[size_t(y - PF) * rs + g * 32] : 0u;
-          p0[g] = rf_step(lo16(c), p0[g], a);
-          p1[g] = rf_step(hi16(c), p1[g], a);
-          const int k2 = g * 64 + lane * 2;
-          if (k2 <= kmax) {
-            const uint32_t c0 = (uint32_t(p0[g] + 32768) << 8) | uint32_t(255 - k2);
-            if (c0 > pk0) { pk1 = pk0; pk0 = c0; } else if (c0 > pk1) { pk1 = c0; }
-          }
-          if (k2 + 1 <= kmax) {
-            const uint32_t c1 = (uint32_t(p1[g] + 32768) << 8) | uint32_t(255 - k2 - 1);
-            if (c1 > pk0) { pk1 = pk0; pk0 = c1; } else if (c1 > pk1) { pk1 = c1; }
-          }
-        }
-        if (y < H - hh) {
-          if (rkey) {
-            const size_t rowo = size_t(y) * W + x - dmin;
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-              const int k2 = g * 64 + lane * 2;
-              if (k2 <= kmax)
-                atomicMax(rkey + rowo - k2, (uint32_t(p0[g] + 32768) << 8) | uint32_t(255 - k2));
-              if (k2 + 1 <= kmax)
-                atomicMax(rkey + rowo - k2 - 1,
-                          (uint32_t(p1[g] + 32768) << 8) | uint32_t(255 - k2 - 1));
+          for (int s = 0; s < KT; ++s) {
+            if (s < nvalid) {
+              const uint32_t key = (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s);
+              const uint32_t lo = min(pk0, key);
+              pk0 = max(pk0, key);
+              pk1 = max(pk1, lo);
             }
           }
+          if (rkey) {
+            const size_t rowo = size_t(y) * W + x - dmin - k0;
 #pragma unroll
-          for (int off = 16; off > 0; off >>= 1) {
-            const uint32_t o0 = __shfl_down_sync(0xffffffffu, pk0, off);
-            const uint32_t o1 = __shfl_down_sync(0xffffffffu, pk1, off);
-            if (o0 > pk0) { pk1 = pk0 > o1 ? pk0 : o1; pk0 = o0; }
-            else if (o0 > pk1) { pk1 = o0; }
+            for (int s = 0; s < KT; ++s)
+              if (s < nvalid)
+                atomicMax(rkey + rowo - s, (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s));
           }
-          const uint32_t w0 = __shfl_sync(0xffffffffu, pk0, 0);
-          const int kw = w0 ? 255 - int(w0 & 255u) : -1;
-          const int km = kw - 1, kp = kw + 1;
-          int32_t mym = -32768, myp = -32768;
+          // this row's costs for the neighbour lookup
 #pragma unroll
-          for (int g = 0; g < G; ++g) {
-            const int k2 = g * 64 + lane * 2;
-            if (k2 <= kmax) { if (k2 == km) mym = p0[g]; if (k2 == kp) myp = p0[g]; }
-            if (k2 + 1 <= kmax) { if (k2 + 1 == km) mym = p1[g]; if (k2 + 1 == kp) myp = p1[g]; }
+          for (int v = 0; v < NV; ++v)
+            reinterpret_cast<uint4*>(rowbuf + k0)[v] =
+                make_uint4(pk16(st[8 * v], st[8 * v + 1]), pk16(st[8 * v + 2], st[8 * v + 3]),
+                           pk16(st[8 * v + 4], st[8 * v + 5]), pk16(st[8 * v + 6], st[8 * v + 7]));
+#pragma unroll
+          for (int off = TPCP / 2; off > 0; off >>= 1) {
+            const uint32_t o0 = __shfl_xor_sync(gmask, pk0, off, TPCP);
+            const uint32_t o1 = __shfl_xor_sync(gmask, pk1, off, TPCP);
+            const uint32_t lo = min(pk0, o0);
+            pk0 = max(pk0, o0);
+            pk1 = max(max(pk1, o1), lo);
           }
-          const int32_t vm = __shfl_sync(0xffffffffu, mym, (km & 63) >> 1);
-          const int32_t vp = __shfl_sync(0xffffffffu, myp, (kp & 63) >> 1);
-          if (lane == 0) {
-            const size_t i = size_t(y) * W;
-            key0[i] = pk0;
-            key1[i] = pk1;
-            const int32_t nm = (kw >= 0 && km >= 0) ? vm : -32768;
-            const int32_t np = (kw >= 0) ? vp : -32768;
-            nbp[i] = pack2(nm, np);
+          __syncwarp(gmask);
+          if (sub == 0) {
+            const int kw = pk0 ? 255 - int(pk0 & 255u) : -1;
+            const int32_t nm = (kw >= 1) ? int32_t(rowbuf[kw - 1]) : -32768;
+            const int32_t np = (kw >= 0 && kw + 1 <= kmax) ? int32_t(rowbuf[kw + 1]) : -32768;
+            const size_t i = size_t(y) * W + x;
+            P.key0[i] = pk0;
+            P.key1[i] = pk1;
+            P.nb[i] = pk16(nm, np);
           }
+          __syncwarp(gmask);
         }
       }
     }
@@ -668,11 +758,17 @@ __global__ void k_export(DevCfg cfg, Batch b) {
   }
 }
 
-size_t rows_smem(int W, int TS, bool packed) {
-  size_t s = size_t(W) * 16 + size_t((W + 7) & ~7) * 2 + size_t(66) * TS * 2;
+size_t rows_smem(int W, int TS, int CP, bool packed) {
+  size_t s = (TS == 16) ? (CP == 2 ? ScoreTable<16, 2>::bytes() : size_t(66) * 16 * 4 * CP)
+                        : ScoreTable<256, 1>::bytes();
+  s += size_t((W + 2) & ~1) * 8 + size_t((W + 1) & ~1) * 8 + size_t((W + 9) & ~7) * 2;
   if (!packed) s += size_t(W) * 2;
   return (s + 15) & ~size_t(15);
 }
+
+int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
+int g_rows_table_copies = 2;      // score-table form: 1 = one 2D table, 8 = eight
+                                  // interleaved copies, 2 = split C1[h] + A1[m]
 
 size_t solve_smem(int W) { return size_t(W) * 53 + 64; }
 
@@ -690,46 +786,80 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+template <bool PACKED, int TS, int CP>
+cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, size_t sm, int threads,
+                          cudaStream_t s) {
+  cudaError_t e = set_smem(k_rows<PACKED, TS, CP>, sm);
+  if (e != cudaSuccess) return e;
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  int fit = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_rows<PACKED, TS, CP>, threads, sm);
+  const int per_sm = std::max(1, std::min(fit > 0 ? fit : 1, g_rows_ctas_per_sm));
+  const int items = b.rows_prefix[b.n];
+  const int grid = std::min(items, per_sm * nsm);
+  k_rows<PACKED, TS, CP><<<grid, threads, sm, s>>>(cfg, b);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int items = b.rows_prefix[b.n];
   if (items == 0) return cudaSuccess;
   int maxW = 0;
   for (int i = 0; i < b.n; ++i) maxW = maxW > b.p[i].W ? maxW : b.p[i].W;
   const int TS = cfg.trunc < 16 ? 16 : 256;
-  const size_t sm = rows_smem(maxW, TS, cfg.packed != 0);
+  const int CP = (TS == 16) ? g_rows_table_copies : 1;
+  const size_t sm = rows_smem(maxW, TS, CP, cfg.packed != 0);
   const int threads = b.maxDpad / 2;
-  cudaError_t e;
-  if (cfg.packed) {
-    if (TS == 16) {
-      if ((e = set_smem(k_rows<true, 16>, sm)) != cudaSuccess) return e;
-      k_rows<true, 16><<<items, threads, sm, s>>>(cfg, b);
-    } else {
-      if ((e = set_smem(k_rows<true, 256>, sm)) != cudaSuccess) return e;
-      k_rows<true, 256><<<items, threads, sm, s>>>(cfg, b);
-    }
-  } else {
-    if (TS == 16) {
-      if ((e = set_smem(k_rows<false, 16>, sm)) != cudaSuccess) return e;
-      k_rows<false, 16><<<items, threads, sm, s>>>(cfg, b);
-    } else {
-      if ((e = set_smem(k_rows<false, 256>, sm)) != cudaSuccess) return e;
-      k_rows<false, 256><<<items, threads, sm, s>>>(cfg, b);
-    }
-  }
+  if (TS == 256)
+    return cfg.packed ? launch_rows_t<true, 256, 1>(cfg, b, sm, threads, s)
+                      : launch_rows_t<false, 256, 1>(cfg, b, sm, threads, s);
+  if (CP == 8)
+    return cfg.packed ? launch_rows_t<true, 16, 8>(cfg, b, sm, threads, s)
+                      : launch_rows_t<false, 16, 8>(cfg, b, sm, threads, s);
+  if (CP == 2)
+    return cfg.packed ? launch_rows_t<true, 16, 2>(cfg, b, sm, threads, s)
+                      : launch_rows_t<false, 16, 2>(cfg, b, sm, threads, s);
+  return cfg.packed ? launch_rows_t<true, 16, 1>(cfg, b, sm, threads, s)
+                    : launch_rows_t<false, 16, 1>(cfg, b, sm, threads, s);
+}
+
+void set_rows_table_copies(int v) { g_rows_table_copies = (v == 8 || v == 2) ? v : 1; }
+int get_rows_table_copies() { return g_rows_table_copies; }
+void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }
+int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
+
+template <int KT, int TPCP>
+cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  const long threads = long(b.cols_prefix[b.n]) * TPCP;
+  const int blocks = int((threads + 255) / 256);
+  k_cols<KT, TPCP><<<blocks, 256, 0, s>>>(cfg, b);
   return cudaGetLastError();
 }
 
+// Lanes per column: Dpad/KT rounded up to a power of two; KT = 16 unless the batch is
+// small, where more, narrower lanes per column buy latency.
+int g_cols_kt = 0;                // 0 = by batch size, else 8 or 16 disparities per lane
+void set_cols_kt(int v) { g_cols_kt = (v == 8 || v == 16) ? v : 0; }
+int get_cols_kt() { return g_cols_kt; }
+
 cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
-  const int warps = b.cols_prefix[b.n];
-  if (warps == 0) return cudaSuccess;
-  const int blocks = (warps * 32 + 255) / 256;
-  switch (b.maxDpad / 64) {
-    case 1: k_cols<1><<<blocks, 256, 0, s>>>(cfg, b); break;
-    case 2: k_cols<2><<<blocks, 256, 0, s>>>(cfg, b); break;
-    case 3: k_cols<3><<<blocks, 256, 0, s>>>(cfg, b); break;
-    default: k_cols<4><<<blocks, 256, 0, s>>>(cfg, b); break;
+  const int cols = b.cols_prefix[b.n];
+  if (cols == 0) return cudaSuccess;
+  const int maxDpad = b.maxDpad;
+  const bool small = g_cols_kt ? g_cols_kt == 8 : long(cols) * maxDpad < 148L * 32 * 16 * 16;
+  if (small || maxDpad <= 64) {
+    switch (maxDpad) {          // KT = 8
+      case 64: return launch_cols_t<8, 8>(cfg, b, s);
+      case 128: return launch_cols_t<8, 16>(cfg, b, s);
+      default: return launch_cols_t<8, 32>(cfg, b, s);
+    }
   }
-  return cudaGetLastError();
+  switch (maxDpad) {            // KT = 16
+    case 128: return launch_cols_t<16, 8>(cfg, b, s);
+    default: return launch_cols_t<16, 16>(cfg, b, s);
+  }
 }
 
 cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref, cudaStream_t s) {

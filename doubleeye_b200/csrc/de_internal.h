@@ -78,6 +78,12 @@ cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref_layout,
                          cudaStream_t s);
+void set_rows_ctas_per_sm(int v);
+int get_rows_ctas_per_sm();
+void set_cols_kt(int v);
+void set_rows_table_copies(int v);
+int get_rows_table_copies();
+int get_cols_kt();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 
 }  // namespace de

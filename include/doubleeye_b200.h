@@ -127,6 +127,29 @@ DE_API int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const 
                         const int* cn, const int16_t* cnb, float* disp, float* margin,
                         float* lrc2, void* stream);
 
+/* Stage timing (a profiling aid; the reference prints the same breakdown from
+ * cudaEvents, core/tools/de_dense_cuda.cu:552-604,847-852).  While enabled, every
+ * de_dense_dev launch set records events on its stream between census, row, column
+ * and solve kernels.  de_stage_times() waits for them, writes the summed ms per
+ * stage into ms[0..n) (n <= 4: census, rows, cols, solve), the number of launch
+ * sets into *launches, and clears them. */
+DE_API int de_stage_timing(int enable);
+DE_API int de_stage_times(float* ms, int n, int* launches);
+
+/* Launch-shape knobs (process-wide; results never depend on them, only speed).
+ * No counterpart in the reference, whose launch shapes are fixed.
+ *   "rows_ctas_per_sm"  cap on row-kernel CTAs resident per SM (default 32, i.e.
+ *                       as many as fit): fewer rows in flight keep each row's
+ *                       forward pass in L2 for its backward pass
+ *   "rows_table_copies" score-table form in shared memory: 1 = one (h, m) table,
+ *                       8 = eight interleaved copies (spreads data-dependent
+ *                       lookups over the banks), 2 = split census and AD tables
+ *                       summed before the shift (default 2)
+ *   "cols_kt"           disparities per lane in the column kernel: 8, 16, or 0 to
+ *                       choose by batch size (default 0) */
+DE_API int de_set_param(const char* name, int value);
+DE_API int de_get_param(const char* name, int* value);
+
 /* confidence() / confidence_u8() of dense_solve.hpp:158-171, host side. */
 DE_API float de_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol);
 

@@ -94,6 +94,7 @@ SIGNATURES = {
                                vp]),
     "de_confidence": (C.c_float, [C.c_float] * 5),
     "de_stage_timing": (C.c_int, [C.c_int]),
+    "de_workspace_status": (C.c_int, [vp, vp, C.POINTER(C.c_int)]),
     "de_set_param": (C.c_int, [C.c_char_p, C.c_int]),
     "de_get_param": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     "de_stage_times": (C.c_int, [C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),

@@ -109,24 +109,31 @@ void make_dev_cfg(const de_cfg& c, DevCfg* o) {
 
 static int dpad_of(int D) { return (D + 63) & ~63; }
 
+static int cpitch_of(int W) { return (W + 2) & ~1; }
+static int apitch_of(int W) { return (W + 8) & ~7; }
+
 size_t pair_workspace_bytes(int W, int H, int D, bool lrc) {
   const size_t WH = size_t(W) * H;
   size_t s = 0;
-  s += align_up(WH * 8) * 2;                      // census words L, R
-  s += align_up(WH * 2) * 2;                      // ax, ay
+  s += align_up(size_t(H) * cpitch_of(W) * 8) * 2;    // census words L, R
+  s += align_up(size_t(H) * apitch_of(W) * 2);        // ax
+  s += align_up(WH * 2);                              // ay
   s += align_up(WH * size_t(dpad_of(D)) * 2);     // filtered volume
   s += align_up(WH * 4) * 3;                      // key0, key1, nb
   if (lrc) s += align_up(WH * 4);                 // reverse-match keys
   return s;
 }
 
-void carve_pair(DevPair* p, void* ws, int W, int H, int D, bool lrc) {
+void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc) {
   const size_t WH = size_t(W) * H;
   uint8_t* c = static_cast<uint8_t*>(ws);
   auto take = [&](size_t bytes) { uint8_t* r = c; c += align_up(bytes); return r; };
-  p->cwL = reinterpret_cast<uint64_t*>(take(WH * 8));
-  p->cwR = reinterpret_cast<uint64_t*>(take(WH * 8));
-  p->ax = reinterpret_cast<uint16_t*>(take(WH * 2));
+  p->cpitch = cpitch_of(W);
+  p->apitch = apitch_of(W);
+  p->lpad = dmin & 1;
+  p->cwL = reinterpret_cast<uint64_t*>(take(size_t(H) * p->cpitch * 8));
+  p->cwR = reinterpret_cast<uint64_t*>(take(size_t(H) * p->cpitch * 8));
+  p->ax = reinterpret_cast<uint16_t*>(take(size_t(H) * p->apitch * 2));
   p->ay = reinterpret_cast<uint16_t*>(take(WH * 2));
   p->vol = reinterpret_cast<int16_t*>(take(WH * size_t(dpad_of(D)) * 2));
   p->key0 = reinterpret_cast<uint32_t*>(take(WH * 4));
@@ -160,15 +167,16 @@ int check_pair(const de_cfg& c, const de_pair& p) {
 
 // Fill one launch set's descriptor table for pairs[first, first+n).
 void fill_batch(const de_cfg& c, const de_pair* pairs, int first, int n, uint8_t* ws,
-                de::Batch* b) {
+                de::Batch* b, int* err) {
   std::memset(b, 0, sizeof(*b));
   b->n = n;
+  b->err = err;
   const int hh = c.census_hh, hw = c.census_hw;
   for (int i = 0; i < n; ++i) {
     const de_pair& p = pairs[first + i];
     const int D = pair_D(c, p);
     de::DevPair& d = b->p[i];
-    de::carve_pair(&d, ws, p.W, p.H, D, c.lrc != 0);
+    de::carve_pair(&d, ws, p.W, p.H, D, c.dmin, c.lrc != 0);
     ws += de::pair_workspace_bytes(p.W, p.H, D, c.lrc != 0);
     d.L = p.L;
     d.R = p.R;
@@ -183,6 +191,9 @@ void fill_batch(const de_cfg& c, const de_pair* pairs, int first, int n, uint8_t
     b->cols_prefix[i + 1] = b->cols_prefix[i] + std::max(0, p.W - 2 * hw - c.dmin);
     b->solve_prefix[i + 1] = b->solve_prefix[i] + p.H;
   }
+  // backward bulk copies of ~4 KB, four deep
+  b->bwd_chunk = std::max(8, 2048 / b->maxDpad);
+  b->bwd_stages = 4;
 }
 
 // Optional stage timing: CUDA events recorded on the launching stream between the
@@ -289,7 +300,7 @@ int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int n,
   int rc = check_cfg(cfg);
   if (rc) return rc;
   if (!bytes || n < 0 || (n > 0 && !pairs)) return fail(DE_ERR_ARG, "bad arguments");
-  size_t s = 0;
+  size_t s = de::kStatusBytes;
   for (int i = 0; i < n; ++i) {
     if ((rc = check_pair(*cfg, pairs[i]))) return rc;
     s += de::pair_workspace_bytes(pairs[i].W, pairs[i].H, pair_D(*cfg, pairs[i]),
@@ -308,12 +319,15 @@ int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace
     return fail(DE_ERR_ARG, "workspace %zu bytes, need %zu", ws_bytes, need);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   uint8_t* ws = static_cast<uint8_t*>(workspace);
+  int* err = reinterpret_cast<int*>(ws);
+  ws += de::kStatusBytes;
+  DE_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
   static de::Batch b;          // large; filled and consumed under the lock
   static std::mutex mu;
   for (int first = 0; first < n; first += de::kMaxBatch) {
     const int m = std::min(de::kMaxBatch, n - first);
     std::lock_guard<std::mutex> lk(mu);
-    fill_batch(*cfg, pairs, first, m, ws, &b);
+    fill_batch(*cfg, pairs, first, m, ws, &b, err);
     for (int i = 0; i < m; ++i)
       ws += de::pair_workspace_bytes(pairs[first + i].W, pairs[first + i].H,
                                      pair_D(*cfg, pairs[first + i]), cfg->lrc != 0);
@@ -337,13 +351,14 @@ int de_census_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, 
   b.n = 1;
   b.p[0].L = L; b.p[0].R = R; b.p[0].cwL = cl; b.p[0].cwR = cr; b.p[0].ax = ax;
   b.p[0].ay = ay; b.p[0].W = W; b.p[0].H = H;
+  b.p[0].cpitch = W; b.p[0].apitch = W; b.p[0].lpad = 0;
   b.pix_prefix[1] = ((W + 31) / 32) * ((H + 7) / 8);
   DE_CUDA(de::launch_census(dc, b, static_cast<cudaStream_t>(stream)));
   return DE_OK;
 }
 
 size_t de_cost_workspace_bytes(int W, int H, int D) {
-  return de::pair_workspace_bytes(W, H, D, false);
+  return de::kStatusBytes + de::pair_workspace_bytes(W, H, D, false);
 }
 
 int de_cost_top2_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
@@ -353,7 +368,7 @@ int de_cost_top2_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int 
   if (rc || (rc = check_dims(W, H))) return rc;
   if (!L || !R || !cs || !cd || !cn) return fail(DE_ERR_ARG, "NULL buffer");
   const int D = cfg->dmax - cfg->dmin + 1;
-  const size_t need = de::pair_workspace_bytes(W, H, D, false);
+  const size_t need = de_cost_workspace_bytes(W, H, D);
   if (ws_bytes < need || !workspace)
     return fail(DE_ERR_ARG, "workspace %zu bytes, need %zu", ws_bytes, need);
   de_cfg c2 = *cfg;
@@ -365,9 +380,11 @@ int de_cost_top2_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int 
   std::lock_guard<std::mutex> lk(mu);
   de_pair p{};
   p.L = L; p.R = R; p.W = W; p.H = H;
-  fill_batch(c2, &p, 0, 1, static_cast<uint8_t*>(workspace), &b);
+  int* err = static_cast<int*>(workspace);
+  fill_batch(c2, &p, 0, 1, static_cast<uint8_t*>(workspace) + de::kStatusBytes, &b, err);
   b.p[0].ref_cs = cs; b.p[0].ref_cd = cd; b.p[0].ref_cn = cn; b.p[0].ref_cnb = cnb;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DE_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
   DE_CUDA(de::launch_census(dc, b, s));
   DE_CUDA(de::launch_rows(dc, b, s));
   DE_CUDA(de::launch_cols(dc, b, s));
@@ -442,6 +459,14 @@ int de_get_param(const char* name, int* value) {
   if (!std::strcmp(name, "cols_kt")) { *value = de::get_cols_kt(); return DE_OK; }
   if (!std::strcmp(name, "rows_table_copies")) { *value = de::get_rows_table_copies(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
+}
+
+int de_workspace_status(const void* workspace, void* stream, int* status) {
+  if (!workspace || !status) return fail(DE_ERR_ARG, "NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  DE_CUDA(cudaMemcpyAsync(status, workspace, sizeof(int), cudaMemcpyDeviceToHost, s));
+  DE_CUDA(cudaStreamSynchronize(s));
+  return DE_OK;
 }
 
 // confidence(), core/include/doubleeye/dense_solve.hpp:158-166.
@@ -589,7 +614,10 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   if (plan.end > plan.out_begin)
     DE_CUDA(cudaMemcpyAsync(Hb + plan.out_begin, Db + plan.out_begin,
                             plan.end - plan.out_begin, cudaMemcpyDeviceToHost, c->stream));
+  int status = 0;
+  DE_CUDA(cudaMemcpyAsync(&status, c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   DE_CUDA(cudaStreamSynchronize(c->stream));
+  if (status) return fail(DE_ERR_TIMEOUT, "a bounded device wait ran out (status %d)", status);
   for (int i = 0; i < n; ++i) {
     const IoLayout& l = plan.p[i];
     const size_t WH = size_t(hp[i].W) * hp[i].H;

@@ -110,10 +110,10 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
     wl |= uint64_t(sL[cy][cx]) << 56;
     wr |= uint64_t(sR[cy][cx]) << 56;
   }
-  P.cwL[i] = wl;
-  P.cwR[i] = wr;
+  P.cwL[size_t(y) * P.cpitch + P.lpad + x] = wl;
+  P.cwR[size_t(y) * P.cpitch + x] = wr;
   const int c = sL[cy][cx];
-  P.ax[i] = x > 0 ? srf[abs(c - int(sL[cy][cx - 1]))] : srf[0];
+  P.ax[size_t(y) * P.apitch + P.lpad + x] = x > 0 ? srf[abs(c - int(sL[cy][cx - 1]))] : srf[0];
   P.ay[i] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
 }
 
@@ -165,151 +165,239 @@ __device__ __forceinline__ int32_t graded(uint64_t lw, uint64_t rw, const void* 
   return static_cast<const int16_t*>(tab)[h * TS + ad];
 }
 
+// Bulk asynchronous copies (cp.async.bulk, the TMA engine's 1-D form) with
+// mbarrier completion.  Every wait is bounded: if a phase never completes the
+// kernel records it in the batch status word and runs on to its end.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return uint32_t(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+constexpr int kWaitLimit = 1 << 22;                  // try_wait rounds before giving up
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
+  for (int i = 0; i < kWaitLimit; ++i)
+    if (mbar_test(bar, parity)) return;
+  if (err) atomicExch(err, 1);
+}
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async;" ::: "memory");
+}
+
+// One row per CTA iteration (the grid is persistent over rows).  The row's census
+// words and x-coefficients arrive by three bulk copies, double-buffered so the next
+// row's inputs load while this row computes.  The forward results go to the volume
+// with plain stores; the backward pass brings them back through a ring of bulk
+// copies (bwd_chunk columns each, bwd_stages deep), so no thread waits on a
+// global load.
 template <bool PACKED, int TS, int CP>
-__global__ void __launch_bounds__(128) k_rows(DevCfg cfg, Batch b) {
-  extern __shared__ __align__(16) uint8_t smem[];
-  // shared layout: table | sL (+1 word pad) | sR | sax (+pad) | sLp | sRp
-  int maxW = 0;
-  for (int i = 0; i < b.n; ++i) maxW = max(maxW, b.p[i].W);
+__global__ void __launch_bounds__(128, 4) k_rows(DevCfg cfg, Batch b) {
+  extern __shared__ __align__(128) uint8_t smem[];
+  __shared__ __align__(8) uint64_t bars[2 + kMaxStages];
+  int cpm = 0, apm = 0, maxW = 0;
+  for (int i = 0; i < b.n; ++i) {
+    cpm = max(cpm, b.p[i].cpitch);
+    apm = max(apm, b.p[i].apitch);
+    maxW = max(maxW, b.p[i].W);
+  }
+  const int CH = b.bwd_chunk, NS = b.bwd_stages, maxDpad = b.maxDpad;
   uint8_t* tabp = smem;
-  uint64_t* sLraw = reinterpret_cast<uint64_t*>(tabp + ScoreTable<TS, CP>::bytes());
-  uint64_t* sR = sLraw + ((maxW + 2) & ~1);
-  uint16_t* saxraw = reinterpret_cast<uint16_t*>(sR + ((maxW + 1) & ~1));
-  uint8_t* sLp = reinterpret_cast<uint8_t*>(saxraw + ((maxW + 9) & ~7));
+  uint8_t* inbuf = tabp + ((ScoreTable<TS, CP>::bytes() + 127) & ~size_t(127));
+  const size_t in_bytes = (size_t(cpm) * 16 + size_t(apm) * 2 + 127) & ~size_t(127);
+  uint8_t* bwdbuf = inbuf + 2 * in_bytes;
+  const size_t stage_bytes = size_t(CH) * maxDpad * 2;
+  uint8_t* sLp = bwdbuf + NS * stage_bytes;
   uint8_t* sRp = sLp + maxW;
-  // table, once per CTA
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    for (int i = 0; i < 2 + NS; ++i) mbar_init(&bars[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
   if (TS == 16 && CP == 2) {
     int32_t* t32 = reinterpret_cast<int32_t*>(tabp);
-    for (int i = threadIdx.x; i < 96; i += blockDim.x)
+    for (int i = tid; i < 96; i += blockDim.x)
       t32[i] = i < 66 ? int32_t(cfg.tbl[i]) * (1024 - cfg.wq)
                       : (i < 82 ? int32_t(cfg.adt[i - 66]) * cfg.wq : 0);
   } else if (TS == 16) {
     int32_t* t32 = reinterpret_cast<int32_t*>(tabp);
-    for (int i = threadIdx.x; i < 66 * 16 * CP; i += blockDim.x) {
+    for (int i = tid; i < 66 * 16 * CP; i += blockDim.x) {
       const int e = i / CP, h = e >> 4, m = e & 15;
       t32[i] = (int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10;
     }
   } else {
     int16_t* t16 = reinterpret_cast<int16_t*>(tabp);
-    for (int i = threadIdx.x; i < 66 * TS; i += blockDim.x) {
+    for (int i = tid; i < 66 * TS; i += blockDim.x) {
       const int h = i / TS, m = i % TS;
       t16[i] = int16_t((int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10);
     }
   }
-  const void* tab = (TS == 16 && CP != 2) ? static_cast<const void*>(reinterpret_cast<const int32_t*>(tabp) + (threadIdx.x % CP))
-                               : static_cast<const void*>(tabp);
+  __syncthreads();
+  const void* tab = (TS == 16 && CP != 2)
+                        ? static_cast<const void*>(reinterpret_cast<const int32_t*>(tabp) + (tid % CP))
+                        : static_cast<const void*>(tabp);
   const int hw = cfg.hw, dmin = cfg.dmin;
-  const int t = threadIdx.x;
-  // sL / sax are offset by (dmin & 1) elements so that x with (x - dmin) even sits on a
-  // 16-byte (sL) / 4-byte (sax) boundary, like sR[x - d] for every lane.
-  uint64_t* sL = sLraw + (dmin & 1);
-  uint16_t* sax = saxraw + (dmin & 1);
   const int total = b.rows_prefix[b.n];
-  for (int item = blockIdx.x; item < total; item += gridDim.x) {
+  int* err = b.err;
+
+  // row inputs of `item` into input buffer `buf` (thread 0 only)
+  auto issue_inputs = [&](int item, int buf) {
+    const int pi = find_pair(b.rows_prefix, b.n, item);
+    const DevPair& P = b.p[pi];
+    const int y = cfg.hh + (item - b.rows_prefix[pi]);
+    uint8_t* dst = inbuf + buf * in_bytes;
+    const uint32_t cb = uint32_t(P.cpitch) * 8, ab = uint32_t(P.apitch) * 2;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // buffer reads done
+    mbar_expect(&bars[buf], 2 * cb + ab);
+    bulk_load(dst, P.cwL + size_t(y) * P.cpitch, cb, &bars[buf]);
+    bulk_load(dst + size_t(cpm) * 8, P.cwR + size_t(y) * P.cpitch, cb, &bars[buf]);
+    bulk_load(dst + size_t(cpm) * 16, P.ax + size_t(y) * P.apitch, ab, &bars[buf]);
+  };
+
+  uint32_t phase = 0;                                 // parity bit per barrier
+  if (tid == 0 && int(blockIdx.x) < total) issue_inputs(blockIdx.x, 0);
+  int it = 0;
+  for (int item = blockIdx.x; item < total; item += gridDim.x, ++it) {
+    const int buf = it & 1;
+    if (tid == 0 && item + int(gridDim.x) < total) issue_inputs(item + gridDim.x, buf ^ 1);
     const int pi = find_pair(b.rows_prefix, b.n, item);
     const DevPair& P = b.p[pi];
     const int W = P.W, Dpad = P.Dpad;
     const int y = cfg.hh + (item - b.rows_prefix[pi]);
     const size_t row = size_t(y) * W;
-    __syncthreads();                                   // previous row's readers are done
-    for (int i = threadIdx.x; i < W; i += blockDim.x) {
-      sL[i] = P.cwL[row + i];
-      sR[i] = P.cwR[row + i];
-      sax[i] = P.ax[row + i];
-      if (!PACKED) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
+    mbar_wait(&bars[buf], (phase >> buf) & 1u, err);
+    phase ^= 1u << buf;
+    const uint8_t* ib = inbuf + buf * in_bytes;
+    const uint64_t* sL = reinterpret_cast<const uint64_t*>(ib) + P.lpad;
+    const uint64_t* sR = reinterpret_cast<const uint64_t*>(ib + size_t(cpm) * 8);
+    const uint16_t* sax = reinterpret_cast<const uint16_t*>(ib + size_t(cpm) * 16) + P.lpad;
+    if (!PACKED) {
+      for (int i = tid; i < W; i += blockDim.x) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
+      __syncthreads();
     }
-    __syncthreads();
-    if (2 * t >= Dpad) continue;
-    const int d0 = dmin + 2 * t;
-    const int xw = hw + dmin + 2 * (t & ~31);          // first lane's start in this warp
-    const int xend = W - hw;                            // scores are 0 from here on
-    uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * Dpad) + t;
-    const size_t xs = size_t(Dpad) >> 1;                // x stride in 32-bit words
+    const bool active = 2 * tid < Dpad;
+    const int d0 = dmin + 2 * tid;
+    const int xw = hw + dmin + 2 * (tid & ~31);       // first lane's start in this warp
+    const int xend = W - hw;                          // scores are 0 from here on
+    uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * Dpad) + tid;
+    const size_t xs = size_t(Dpad) >> 1;              // x stride in 32-bit words
     int32_t f0 = 0, f1 = 0;
-    uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;   // chain k1's word
-    int x = xw;
-    // ramp: lanes may not have reached their own valid start yet; ends on an x with
-    // (x - dmin) even so the paired loop below is aligned
-    int xramp = min(xend, xw + 64);
-    xramp += (xramp - dmin) & 1;
-    xramp = min(xramp, xend);
-    for (; x < xramp; ++x) {
-      const int32_t a = sax[x];
-      const uint64_t lw = sL[x];
-      int32_t v0 = 0, v1 = 0;
-      uint64_t rw = 0;
-      if (x - d0 >= hw) {
-        rw = sR[x - d0];
-        v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
+    if (active) {
+      uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;  // chain k1's word
+      int x = xw;
+      int xramp = min(xend, xw + 64);                 // lanes may still be before their start
+      xramp += (xramp - dmin) & 1;                    // the paired loop needs x - dmin even
+      xramp = min(xramp, xend);
+      for (; x < xramp; ++x) {
+        const int32_t a = sax[x];
+        const uint64_t lw = sL[x];
+        int32_t v0 = 0, v1 = 0;
+        uint64_t rw = 0;
+        if (x - d0 >= hw) {
+          rw = sR[x - d0];
+          v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
+        }
+        if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
+        rprev = rw;
+        f0 = rf_step(v0, f0, a);
+        f1 = rf_step(v1, f1, a);
+        out[x * xs] = pack2(f0, f1);
       }
-      if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
-      rprev = rw;
-      f0 = rf_step(v0, f0, a);
-      f1 = rf_step(v1, f1, a);
-      out[x * xs] = pack2(f0, f1);
-    }
-    // main: two x per iteration, every chain in the warp inside its window
 #pragma unroll 2
-    for (; x + 1 < xend; x += 2) {
-      const uint32_t a2 = *reinterpret_cast<const uint32_t*>(sax + x);
-      const ulonglong2 l2 = *reinterpret_cast<const ulonglong2*>(sL + x);
-      const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(sR + (x - d0));
-      const int32_t a0 = int32_t(a2 & 0xFFFFu), a1 = int32_t(a2 >> 16);
-      // x:   chain0 <- r2.x (x - d0), chain1 <- rprev (x - d0 - 1)
-      // x+1: chain0 <- r2.y,          chain1 <- r2.x
-      const int32_t v00 = graded<PACKED, TS, CP>(l2.x, r2.x, tab, sLp, sRp, x, x - d0);
-      const int32_t v01 = graded<PACKED, TS, CP>(l2.x, rprev, tab, sLp, sRp, x, x - d0 - 1);
-      const int32_t v10 = graded<PACKED, TS, CP>(l2.y, r2.y, tab, sLp, sRp, x + 1, x + 1 - d0);
-      const int32_t v11 = graded<PACKED, TS, CP>(l2.y, r2.x, tab, sLp, sRp, x + 1, x - d0);
-      rprev = r2.y;
-      f0 = rf_step(v00, f0, a0);
-      f1 = rf_step(v01, f1, a0);
-      out[x * xs] = pack2(f0, f1);
-      f0 = rf_step(v10, f0, a1);
-      f1 = rf_step(v11, f1, a1);
-      out[(x + 1) * xs] = pack2(f0, f1);
+      for (; x + 1 < xend; x += 2) {                  // two x per iteration
+        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(sax + x);
+        const ulonglong2 l2 = *reinterpret_cast<const ulonglong2*>(sL + x);
+        const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(sR + (x - d0));
+        const int32_t a0 = int32_t(a2 & 0xFFFFu), a1 = int32_t(a2 >> 16);
+        const int32_t v00 = graded<PACKED, TS, CP>(l2.x, r2.x, tab, sLp, sRp, x, x - d0);
+        const int32_t v01 = graded<PACKED, TS, CP>(l2.x, rprev, tab, sLp, sRp, x, x - d0 - 1);
+        const int32_t v10 = graded<PACKED, TS, CP>(l2.y, r2.y, tab, sLp, sRp, x + 1, x + 1 - d0);
+        const int32_t v11 = graded<PACKED, TS, CP>(l2.y, r2.x, tab, sLp, sRp, x + 1, x - d0);
+        rprev = r2.y;
+        f0 = rf_step(v00, f0, a0);
+        f1 = rf_step(v01, f1, a0);
+        out[x * xs] = pack2(f0, f1);
+        f0 = rf_step(v10, f0, a1);
+        f1 = rf_step(v11, f1, a1);
+        out[(x + 1) * xs] = pack2(f0, f1);
+      }
+      for (; x < xend; ++x) {                         // at most one leftover step
+        const int32_t a = sax[x];
+        const uint64_t lw = sL[x];
+        const uint64_t rw = sR[x - d0];
+        const int32_t v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
+        const int32_t v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
+        rprev = rw;
+        f0 = rf_step(v0, f0, a);
+        f1 = rf_step(v1, f1, a);
+        out[x * xs] = pack2(f0, f1);
+      }
+      for (; x < W; ++x) {                            // right border, score 0
+        const int32_t a = sax[x];
+        f0 = rf_step(0, f0, a);
+        f1 = rf_step(0, f1, a);
+        out[x * xs] = pack2(f0, f1);
+      }
     }
-    for (; x < xend; ++x) {                          // at most one leftover step
-      const int32_t a = sax[x];
-      const uint64_t lw = sL[x];
-      const uint64_t rw = sR[x - d0];
-      const int32_t v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
-      const int32_t v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
-      rprev = rw;
-      f0 = rf_step(v0, f0, a);
-      f1 = rf_step(v1, f1, a);
-      out[x * xs] = pack2(f0, f1);
-    }
-    for (; x < W; ++x) {                             // right border, score 0
-      const int32_t a = sax[x];
-      f0 = rf_step(0, f0, a);
-      f1 = rf_step(0, f1, a);
-      out[x * xs] = pack2(f0, f1);
-    }
-    // backward: seed with the forward value at W-1 (already stored), coefficient at
-    // x+1; the forward results come back through L2, prefetched PF columns ahead
-    int32_t g0 = f0, g1 = f1;
-    const int xlo = xw;
-    x = W - 2;
-    constexpr int PF = 32;
-    uint32_t ring[PF];
-#pragma unroll
-    for (int j = 0; j < PF; ++j) ring[j] = (x - j >= xlo) ? out[(x - j) * xs] : 0u;
-    while (x >= xlo) {
-#pragma unroll
-      for (int j = 0; j < PF; ++j) {
-        const int xx = x - j;
-        if (xx >= xlo) {
-          const uint32_t c = ring[j];
-          const int32_t a = sax[xx + 1];
+    // backward: forward results come back by bulk copy, chunk by chunk from the right
+    fence_proxy_async();                              // our stores before the async reads
+    __syncthreads();
+    const int xlo_cta = hw + dmin;
+    const int jmax = (W - 2) / CH, jmin = xlo_cta / CH;
+    auto issue_chunk = [&](int j, int slot) {
+      const int xa = j * CH;
+      const uint32_t bytes = uint32_t(min(CH, W - xa)) * uint32_t(Dpad) * 2u;
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // stage reads done
+      mbar_expect(&bars[2 + slot], bytes);
+      bulk_load(bwdbuf + slot * stage_bytes, P.vol + (row + xa) * Dpad, bytes, &bars[2 + slot]);
+    };
+    if (tid == 0)
+      for (int q = 0; q < NS && jmax - q >= jmin; ++q) issue_chunk(jmax - q, q);
+    int32_t g0 = f0, g1 = f1;                         // seed: forward value at W-1
+    int slot = 0;
+    for (int j = jmax; j >= jmin; --j) {
+      mbar_wait(&bars[2 + slot], (phase >> (2 + slot)) & 1u, err);
+      phase ^= 1u << (2 + slot);
+      if (active) {
+        const int xa = j * CH;
+        const uint32_t* cb = reinterpret_cast<const uint32_t*>(bwdbuf + slot * stage_bytes) + tid;
+        const int xlo = max(xa, xw);
+        for (int x = min(W - 2, xa + CH - 1); x >= xlo; --x) {
+          const uint32_t c = cb[(x - xa) * xs];
+          const int32_t a = sax[x + 1];
           g0 = rf_step(lo16(c), g0, a);
           g1 = rf_step(hi16(c), g1, a);
-          ring[j] = (xx - PF >= xlo) ? out[(xx - PF) * xs] : 0u;
-          out[xx * xs] = pack2(g0, g1);
+          out[x * xs] = pack2(g0, g1);
         }
       }
-      x -= PF;
+      __syncthreads();                                // stage consumed by every thread
+      if (tid == 0 && j - NS >= jmin) issue_chunk(j - NS, slot);
+      slot = (slot + 1 == NS) ? 0 : slot + 1;
     }
+    __syncthreads();                                  // input buffer free for reuse
   }
 }
 
@@ -519,7 +607,7 @@ __device__ __forceinline__ void block_excl_scan(int* a, int n, int* warp_sums) {
 
 template <bool REF_LAYOUT>
 __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
-  extern __shared__ __align__(16) uint8_t smem[];
+  extern __shared__ __align__(128) uint8_t smem[];
   const int item = blockIdx.x;
   const int pi = find_pair(b.solve_prefix, b.n, item);
   const DevPair& P = b.p[pi];
@@ -758,11 +846,19 @@ __global__ void k_export(DevCfg cfg, Batch b) {
   }
 }
 
-size_t rows_smem(int W, int TS, int CP, bool packed) {
-  size_t s = (TS == 16) ? (CP == 2 ? ScoreTable<16, 2>::bytes() : size_t(66) * 16 * 4 * CP)
-                        : ScoreTable<256, 1>::bytes();
-  s += size_t((W + 2) & ~1) * 8 + size_t((W + 1) & ~1) * 8 + size_t((W + 9) & ~7) * 2;
-  if (!packed) s += size_t(W) * 2;
+size_t rows_smem(const Batch& b, int TS, int CP, bool packed) {
+  int cpm = 0, apm = 0, maxW = 0;
+  for (int i = 0; i < b.n; ++i) {
+    cpm = std::max(cpm, b.p[i].cpitch);
+    apm = std::max(apm, b.p[i].apitch);
+    maxW = std::max(maxW, b.p[i].W);
+  }
+  size_t tab = (TS == 16) ? (CP == 2 ? ScoreTable<16, 2>::bytes() : size_t(66) * 16 * 4 * CP)
+                          : ScoreTable<256, 1>::bytes();
+  size_t s = (tab + 127) & ~size_t(127);
+  s += 2 * ((size_t(cpm) * 16 + size_t(apm) * 2 + 127) & ~size_t(127));
+  s += size_t(b.bwd_stages) * b.bwd_chunk * b.maxDpad * 2;
+  if (!packed) s += size_t(maxW) * 2;
   return (s + 15) & ~size_t(15);
 }
 
@@ -806,11 +902,9 @@ cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, size_t sm, int thre
 cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int items = b.rows_prefix[b.n];
   if (items == 0) return cudaSuccess;
-  int maxW = 0;
-  for (int i = 0; i < b.n; ++i) maxW = maxW > b.p[i].W ? maxW : b.p[i].W;
   const int TS = cfg.trunc < 16 ? 16 : 256;
   const int CP = (TS == 16) ? g_rows_table_copies : 1;
-  const size_t sm = rows_smem(maxW, TS, CP, cfg.packed != 0);
+  const size_t sm = rows_smem(b, TS, CP, cfg.packed != 0);
   const int threads = b.maxDpad / 2;
   if (TS == 256)
     return cfg.packed ? launch_rows_t<true, 256, 1>(cfg, b, sm, threads, s)

@@ -22,10 +22,10 @@ constexpr int kMaxH = 8192;
 struct DevPair {
   const uint8_t* L;
   const uint8_t* R;
-  uint64_t* cwL;       // census word | pixel << 56 (7x7) or census only (wider windows)
-  uint64_t* cwR;
-  uint16_t* ax;        // Q15 filter coefficients of L, x direction
-  uint16_t* ay;        // ... y direction
+  uint64_t* cwL;       // census word | pixel << 56 (7x7) or census only (wider windows);
+  uint64_t* cwR;       //   element (y, x) at [y*cpitch + lpad + x] (left), [y*cpitch + x]
+  uint16_t* ax;        // Q15 filter coefficients of L, x direction, [y*apitch + lpad + x]
+  uint16_t* ay;        // ... y direction, [y*W + x]
   int16_t* vol;        // [H][W][Dpad] filtered cost, int16 (Q14)
   uint32_t* key0;      // packed top-2 keys, (v + 32768) << 8 | (255 - k); 0 = empty
   uint32_t* key1;
@@ -42,6 +42,9 @@ struct DevPair {
   int* ref_cn;
   int16_t* ref_cnb;
   int W, H, D, Dpad;
+  int cpitch;          // census row pitch in words (even: rows start 16-byte aligned)
+  int apitch;          // ax row pitch in elements (multiple of 8)
+  int lpad;            // left-row front pad (dmin & 1) so paired loads stay aligned
 };
 
 // Arithmetic configuration, precomputed on the host from de_cfg.
@@ -60,6 +63,9 @@ struct DevCfg {
 struct Batch {
   int n;
   int maxDpad;
+  int bwd_chunk;       // row kernel: x columns per backward bulk copy
+  int bwd_stages;      // ... ring depth
+  int* err;            // device status word (bounded waits that ran out set it)
   int rows_prefix[kMaxBatch + 1];   // row-kernel work items (rows in [hh, H-hh))
   int cols_prefix[kMaxBatch + 1];   // column-kernel work items (cols with candidates)
   int solve_prefix[kMaxBatch + 1];  // solve work items (all rows)
@@ -70,7 +76,9 @@ struct Batch {
 // Host-side preparation (de_capi.cu).
 void make_dev_cfg(const de_cfg& c, DevCfg* out);
 size_t pair_workspace_bytes(int W, int H, int D, bool lrc);
-void carve_pair(DevPair* p, void* ws, int W, int H, int D, bool lrc);
+void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc);
+constexpr int kMaxStages = 8;
+constexpr size_t kStatusBytes = 256;   // head of every dense workspace
 
 // Launchers (de_dense.cu).  All enqueue on `stream` and return the launch status.
 cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s);

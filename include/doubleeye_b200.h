@@ -97,7 +97,8 @@ typedef struct de_pair {
   float* cand;
 } de_pair;
 
-/* Workspace for de_dense_dev on n pairs (sum over pairs, 256-byte aligned). */
+/* Workspace for de_dense_dev on n pairs (sum over pairs, 256-byte aligned, plus a
+ * 256-byte status head). */
 DE_API int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int n,
                                     size_t* bytes);
 /* Census -> cost -> filter -> top-2 -> row solve for n pairs in one set of
@@ -106,6 +107,11 @@ DE_API int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int
  * (core/tools/de_dense_cuda.cu:556-663). */
 DE_API int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n,
                         void* workspace, size_t ws_bytes, void* stream);
+
+/* Status of the last launch set that used this workspace: waits for the stream,
+ * then writes 0, or non-zero if a bounded device wait ran out (the results of that
+ * launch set are then invalid).  The host-pointer context checks it itself. */
+DE_API int de_workspace_status(const void* workspace, void* stream, int* status);
 
 /* Stage entry points, for stage-level parity and for callers that keep their
  * own pipeline.  Census planes: cl/cr u64 (0 on the border), ax/ay u16 Q15

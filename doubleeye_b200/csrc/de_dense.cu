@@ -423,38 +423,57 @@ __device__ __forceinline__ uint32_t pk16(int32_t lo, int32_t hi) {
 }
 
 template <int KT, int TPCP>
-__global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
+__global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b, int nstages) {
   static_assert(KT % 8 == 0 && TPCP >= 1 && TPCP <= 32, "shape");
-  constexpr int NV = KT / 8;                         // 128-bit vectors per row
-  constexpr int PF = 4;                              // rows prefetched ahead
+  constexpr int NV = KT / 8;                         // 128-bit vectors per row per lane
+  constexpr int NCOL = 256 / TPCP;                   // columns per CTA tile
+  constexpr int PFA = 8;                             // ay rows prefetched ahead
+  extern __shared__ __align__(128) uint8_t smem[];   // nstages x NCOL x maxDpad int16
   __shared__ __align__(16) int16_t sbuf[256 / 32][32 * KT];
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int group = (blockIdx.x * blockDim.x + threadIdx.x) / TPCP;
-  const int sub = lane % TPCP, gbase = lane - sub;
+  __shared__ __align__(8) uint64_t bars[kMaxStages];
+  const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
+  const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
   const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
-  if (group >= b.cols_prefix[b.n]) return;           // whole groups leave together
-  const int pi = find_pair(b.cols_prefix, b.n, group);
+  const int tile = blockIdx.x;                        // cols_prefix counts tiles here
+  const int pi = find_pair(b.cols_prefix, b.n, tile);
   const DevPair& P = b.p[pi];
   const int W = P.W, H = P.H, D = P.D, Dpad = P.Dpad;
   const int hw = cfg.hw, hh = cfg.hh, dmin = cfg.dmin;
-  const int x = hw + dmin + (group - b.cols_prefix[pi]);
-  const int kmax = min(D - 1, x - hw - dmin);
+  const int xbase = hw + dmin + (tile - b.cols_prefix[pi]) * NCOL;
+  const int ncols = min(NCOL, W - hw - xbase);        // columns with candidates
+  const int ccopy = min(NCOL, W - xbase);             // columns moved per row
+  const uint32_t row_bytes = uint32_t(ccopy) * uint32_t(Dpad) * 2u;
+  const size_t stage_bytes = size_t(NCOL) * b.maxDpad * 2;
+  const int NS = nstages;
+  const int x = xbase + gi;
   const int k0 = sub * KT;
-  const bool live = k0 < Dpad;                       // lanes past this pair's Dpad idle
+  const bool colok = gi < ncols;
+  const bool live = colok && k0 < Dpad;
+  const int kmax = colok ? min(D - 1, x - hw - dmin) : -1;
   const int nvalid = max(0, min(KT, kmax - k0 + 1));
-  uint4* col = reinterpret_cast<uint4*>(P.vol + size_t(x) * Dpad + (live ? k0 : 0));
-  const size_t rs = size_t(W) * Dpad / 8;            // row stride in uint4
-  const uint16_t* ay = P.ay + x;
-  const int yin = H - hh;                            // rows >= yin have zero input
+  const int yin = H - hh;                             // rows >= yin have zero input
+  int* err = b.err;
+  if (tid == 0) {
+    for (int i = 0; i < NS; ++i) mbar_init(&bars[i], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const int16_t* volt = P.vol + size_t(xbase) * Dpad;          // this tile, row 0
+  const size_t rowstride = size_t(W) * Dpad;                    // int16 per image row
+  auto issue = [&](int y, int stg) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(&bars[stg], row_bytes);
+    bulk_load(smem + stg * stage_bytes, volt + size_t(y) * rowstride, row_bytes, &bars[stg]);
+  };
+  auto read_stage = [&](int stg, uint4* dst) {
+    const uint4* src = reinterpret_cast<const uint4*>(smem + stg * stage_bytes +
+                                                      (size_t(gi) * Dpad + k0) * 2);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) dst[v] = live ? src[v] : make_uint4(0, 0, 0, 0);
+  };
   int32_t st[KT];
 #pragma unroll
   for (int s = 0; s < KT; ++s) st[s] = 0;
-  uint4 ring[PF][NV];
-  auto load_row = [&](int y, uint4* dst) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-      dst[v] = (live && y >= hh && y < yin) ? col[size_t(y) * rs + v] : make_uint4(0, 0, 0, 0);
-  };
   auto step = [&](const uint4* src, int32_t a) {
 #pragma unroll
     for (int v = 0; v < NV; ++v) {
@@ -466,45 +485,72 @@ __global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
       }
     }
   };
-  // ---- forward, rows hh..H-1 (rows < hh are zero and leave the carry at 0) ----
+  auto packed = [&](int v) {
+    return make_uint4(pk16(st[8 * v], st[8 * v + 1]), pk16(st[8 * v + 2], st[8 * v + 3]),
+                      pk16(st[8 * v + 4], st[8 * v + 5]), pk16(st[8 * v + 6], st[8 * v + 7]));
+  };
+  uint4* gcol = reinterpret_cast<uint4*>(P.vol + size_t(x) * Dpad + (live ? k0 : 0));
+  const size_t grs = rowstride / 8;                   // image-row stride in uint4
+  const uint16_t* ay = P.ay + (colok ? x : xbase);
+  uint32_t phase = 0;
+  // ---- vertical forward, rows hh..H-1, results stored in place --------------------
+  if (tid == 0)
+    for (int q = 0; q < NS && hh + q < yin; ++q) issue(hh + q, q);
+  int32_t aring[PFA];
 #pragma unroll
-  for (int j = 0; j < PF; ++j) load_row(hh + j, ring[j]);
-  for (int y0 = hh; y0 < H; y0 += PF) {
+  for (int j = 0; j < PFA; ++j) aring[j] = (hh + j < H) ? ay[size_t(hh + j) * W] : 0;
+  int stg = 0;
+  for (int y0 = hh; y0 < H; y0 += PFA) {
 #pragma unroll
-    for (int j = 0; j < PF; ++j) {
+    for (int j = 0; j < PFA; ++j) {
       const int y = y0 + j;
       if (y < H) {
-        const int32_t a = ay[size_t(y) * W];
-        step(ring[j], a);
-        load_row(y + PF, ring[j]);
+        const int32_t a = aring[j];
+        aring[j] = (y + PFA < H) ? ay[size_t(y + PFA) * W] : 0;
+        uint4 c[NV];
+        if (y < yin) {
+          mbar_wait(&bars[stg], (phase >> stg) & 1u, err);
+          phase ^= 1u << stg;
+          read_stage(stg, c);
+        } else {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) c[v] = make_uint4(0, 0, 0, 0);
+        }
+        step(c, a);
         if (live) {
 #pragma unroll
-          for (int v = 0; v < NV; ++v)
-            col[size_t(y) * rs + v] =
-                make_uint4(pk16(st[8 * v], st[8 * v + 1]), pk16(st[8 * v + 2], st[8 * v + 3]),
-                           pk16(st[8 * v + 4], st[8 * v + 5]), pk16(st[8 * v + 6], st[8 * v + 7]));
+          for (int v = 0; v < NV; ++v) gcol[size_t(y) * grs + v] = packed(v);
+        }
+        if (y < yin) {
+          __syncthreads();                            // stage consumed
+          if (tid == 0 && y + NS < yin) issue(y + NS, stg);
+          stg = (stg + 1 == NS) ? 0 : stg + 1;
         }
       }
     }
   }
-  // ---- backward from H-1 (its value is the forward one), coefficient at y+1 ----
-  auto load_fwd = [&](int y, uint4* dst) {            // rows written by the forward pass
+  // ---- vertical backward from H-1 (its value is the forward one) + top-2 ----------
+  fence_proxy_async();
+  __syncthreads();
+  if (tid == 0)
+    for (int q = 0; q < NS && H - 2 - q >= hh; ++q) issue(H - 2 - q, q);
 #pragma unroll
-    for (int v = 0; v < NV; ++v)
-      dst[v] = (live && y >= hh) ? col[size_t(y) * rs + v] : make_uint4(0, 0, 0, 0);
-  };
-#pragma unroll
-  for (int j = 0; j < PF; ++j) load_fwd(H - 2 - j, ring[j]);
+  for (int j = 0; j < PFA; ++j) aring[j] = (H - 1 - j >= hh + 1) ? ay[size_t(H - 1 - j) * W] : 0;
   uint32_t* rkey = P.rkey;
   int16_t* rowbuf = &sbuf[wib][gbase * KT];
-  for (int y0 = H - 2; y0 >= hh; y0 -= PF) {
+  stg = 0;
+  for (int y0 = H - 2; y0 >= hh; y0 -= PFA) {
 #pragma unroll
-    for (int j = 0; j < PF; ++j) {
+    for (int j = 0; j < PFA; ++j) {
       const int y = y0 - j;
       if (y >= hh) {
-        const int32_t a = ay[size_t(y + 1) * W];
-        step(ring[j], a);
-        load_fwd(y - PF, ring[j]);
+        const int32_t a = aring[j];                   // coefficient at y + 1
+        aring[j] = (y + 1 - PFA >= hh + 1) ? ay[size_t(y + 1 - PFA) * W] : 0;
+        mbar_wait(&bars[stg], (phase >> stg) & 1u, err);
+        phase ^= 1u << stg;
+        uint4 c[NV];
+        read_stage(stg, c);
+        step(c, a);
         if (y < yin) {
           uint32_t pk0 = 0, pk1 = 0;
 #pragma unroll
@@ -523,12 +569,8 @@ __global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
               if (s < nvalid)
                 atomicMax(rkey + rowo - s, (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s));
           }
-          // this row's costs for the neighbour lookup
 #pragma unroll
-          for (int v = 0; v < NV; ++v)
-            reinterpret_cast<uint4*>(rowbuf + k0)[v] =
-                make_uint4(pk16(st[8 * v], st[8 * v + 1]), pk16(st[8 * v + 2], st[8 * v + 3]),
-                           pk16(st[8 * v + 4], st[8 * v + 5]), pk16(st[8 * v + 6], st[8 * v + 7]));
+          for (int v = 0; v < NV; ++v) reinterpret_cast<uint4*>(rowbuf + k0)[v] = packed(v);
 #pragma unroll
           for (int off = TPCP / 2; off > 0; off >>= 1) {
             const uint32_t o0 = __shfl_xor_sync(gmask, pk0, off, TPCP);
@@ -538,7 +580,7 @@ __global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
             pk1 = max(max(pk1, o1), lo);
           }
           __syncwarp(gmask);
-          if (sub == 0) {
+          if (sub == 0 && colok) {
             const int kw = pk0 ? 255 - int(pk0 & 255u) : -1;
             const int32_t nm = (kw >= 1) ? int32_t(rowbuf[kw - 1]) : -32768;
             const int32_t np = (kw >= 0 && kw + 1 <= kmax) ? int32_t(rowbuf[kw + 1]) : -32768;
@@ -547,8 +589,10 @@ __global__ void __launch_bounds__(256) k_cols(DevCfg cfg, Batch b) {
             P.key1[i] = pk1;
             P.nb[i] = pk16(nm, np);
           }
-          __syncwarp(gmask);
         }
+        __syncthreads();                              // stage and row buffer consumed
+        if (tid == 0 && y - NS >= hh) issue(y - NS, stg);
+        stg = (stg + 1 == NS) ? 0 : stg + 1;
       }
     }
   }
@@ -862,6 +906,8 @@ size_t rows_smem(const Batch& b, int TS, int CP, bool packed) {
   return (s + 15) & ~size_t(15);
 }
 
+struct de_cfg_hw { int hw, dmin; };
+int g_cols_stage_kb = 32;         // column kernel: shared bytes for the row ring
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
 int g_rows_table_copies = 2;      // score-table form: 1 = one 2D table, 8 = eight
                                   // interleaved copies, 2 = split C1[h] + A1[m]
@@ -925,34 +971,51 @@ void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }
 int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
 
 template <int KT, int TPCP>
-cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
-  const long threads = long(b.cols_prefix[b.n]) * TPCP;
-  const int blocks = int((threads + 255) / 256);
-  k_cols<KT, TPCP><<<blocks, 256, 0, s>>>(cfg, b);
+cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& hwc,
+                          cudaStream_t s) {
+  constexpr int NCOL = 256 / TPCP;
+  thread_local Batch b;                               // tiles instead of columns
+  b = b0;
+  b.cols_prefix[0] = 0;
+  for (int i = 0; i < b.n; ++i) {
+    const int ncols = std::max(0, b.p[i].W - 2 * hwc.hw - hwc.dmin);
+    b.cols_prefix[i + 1] = b.cols_prefix[i] + (ncols + NCOL - 1) / NCOL;
+  }
+  const int tiles = b.cols_prefix[b.n];
+  if (tiles == 0) return cudaSuccess;
+  const size_t stage = size_t(NCOL) * b.maxDpad * 2;
+  const int ns = int(std::max<size_t>(3, std::min<size_t>(kMaxStages, g_cols_stage_kb * 1024 / stage)));
+  const size_t sm = stage * ns;
+  cudaError_t e = set_smem(k_cols<KT, TPCP>, sm);
+  if (e != cudaSuccess) return e;
+  k_cols<KT, TPCP><<<tiles, 256, sm, s>>>(cfg, b, ns);
   return cudaGetLastError();
 }
 
-// Lanes per column: Dpad/KT rounded up to a power of two; KT = 16 unless the batch is
-// small, where more, narrower lanes per column buy latency.
 int g_cols_kt = 0;                // 0 = by batch size, else 8 or 16 disparities per lane
 void set_cols_kt(int v) { g_cols_kt = (v == 8 || v == 16) ? v : 0; }
 int get_cols_kt() { return g_cols_kt; }
+void set_cols_stage_kb(int v) { g_cols_stage_kb = v < 4 ? 4 : (v > 160 ? 160 : v); }
+int get_cols_stage_kb() { return g_cols_stage_kb; }
 
+// Lanes per column: Dpad/KT rounded up to a power of two; KT = 16 unless the batch is
+// small, where more, narrower lanes per column buy parallelism.
 cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  if (b.cols_prefix[b.n] == 0) return cudaSuccess;
+  const de_cfg_hw hwc{cfg.hw, cfg.dmin};
   const int cols = b.cols_prefix[b.n];
-  if (cols == 0) return cudaSuccess;
   const int maxDpad = b.maxDpad;
   const bool small = g_cols_kt ? g_cols_kt == 8 : long(cols) * maxDpad < 148L * 32 * 16 * 16;
   if (small || maxDpad <= 64) {
     switch (maxDpad) {          // KT = 8
-      case 64: return launch_cols_t<8, 8>(cfg, b, s);
-      case 128: return launch_cols_t<8, 16>(cfg, b, s);
-      default: return launch_cols_t<8, 32>(cfg, b, s);
+      case 64: return launch_cols_t<8, 8>(cfg, b, hwc, s);
+      case 128: return launch_cols_t<8, 16>(cfg, b, hwc, s);
+      default: return launch_cols_t<8, 32>(cfg, b, hwc, s);
     }
   }
   switch (maxDpad) {            // KT = 16
-    case 128: return launch_cols_t<16, 8>(cfg, b, s);
-    default: return launch_cols_t<16, 16>(cfg, b, s);
+    case 128: return launch_cols_t<16, 8>(cfg, b, hwc, s);
+    default: return launch_cols_t<16, 16>(cfg, b, hwc, s);
   }
 }
 

@@ -77,7 +77,7 @@ struct Batch {
 void make_dev_cfg(const de_cfg& c, DevCfg* out);
 size_t pair_workspace_bytes(int W, int H, int D, bool lrc);
 void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc);
-constexpr int kMaxStages = 8;
+constexpr int kMaxStages = 16;
 constexpr size_t kStatusBytes = 256;   // head of every dense workspace
 
 // Launchers (de_dense.cu).  All enqueue on `stream` and return the launch status.
@@ -89,6 +89,8 @@ cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref_layout
 void set_rows_ctas_per_sm(int v);
 int get_rows_ctas_per_sm();
 void set_cols_kt(int v);
+void set_cols_stage_kb(int v);
+int get_cols_stage_kb();
 void set_rows_table_copies(int v);
 int get_rows_table_copies();
 int get_cols_kt();

@@ -89,7 +89,7 @@ void make_dev_cfg(const de_cfg& c, DevCfg* o) {
   o->min_margin = c.min_margin;
   o->min_ratio = c.min_ratio;
   const int nbits = census_bits(c);
-  o->packed = nbits <= 56;
+  o->packed = nbits <= 48;
   const int half = nbits / 2;
   for (int h = 0; h <= 2 * half && h < 66; ++h)
     o->tbl[h] = int16_t(((half - h) * 16384) / half);
@@ -193,7 +193,7 @@ void fill_batch(const de_cfg& c, const de_pair* pairs, int first, int n, uint8_t
   }
   // backward bulk copies of ~4 KB, four deep
   b->bwd_chunk = std::max(8, 2048 / b->maxDpad);
-  b->bwd_stages = 4;
+  b->bwd_stages = 3;
 }
 
 // Optional stage timing: CUDA events recorded on the launching stream between the
@@ -449,7 +449,6 @@ int de_set_param(const char* name, int value) {
   if (!name) return fail(DE_ERR_ARG, "name is NULL");
   if (!std::strcmp(name, "rows_ctas_per_sm")) { de::set_rows_ctas_per_sm(value); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { de::set_cols_kt(value); return DE_OK; }
-  if (!std::strcmp(name, "rows_table_copies")) { de::set_rows_table_copies(value); return DE_OK; }
   if (!std::strcmp(name, "cols_stage_kb")) { de::set_cols_stage_kb(value); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
@@ -458,7 +457,6 @@ int de_get_param(const char* name, int* value) {
   if (!name || !value) return fail(DE_ERR_ARG, "NULL argument");
   if (!std::strcmp(name, "rows_ctas_per_sm")) { *value = de::get_rows_ctas_per_sm(); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { *value = de::get_cols_kt(); return DE_OK; }
-  if (!std::strcmp(name, "rows_table_copies")) { *value = de::get_rows_table_copies(); return DE_OK; }
   if (!std::strcmp(name, "cols_stage_kb")) { *value = de::get_cols_stage_kb(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }

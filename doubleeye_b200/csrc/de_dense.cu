@@ -66,6 +66,53 @@ __device__ __forceinline__ int32_t hi16(uint32_t v) { return int32_t(int16_t(v >
 // core/tools/de_dense.cpp:94-129,186-227 (census), :531-561 (rf_coeffs).
 constexpr int kCTX = 32, kCTY = 8, kMaxHalf = 4;
 
+// Packed census words (windows of <= 48 bits): lo32 = bits 0..31; hi32 = bits
+// 32..47 | guard bit 19 (left words only) | pixel byte at bits 20..27.  Then
+// (left.hi - right.hi) >> 20 is exactly L - R: the guard keeps the census bits from
+// borrowing into the pixel field.  (left ^ right) masked to the census bits gives the
+// Hamming input as before.
+constexpr uint32_t kCensusHiMask = 0xFFFFu;
+constexpr uint32_t kGuard = 1u << 19;
+constexpr int kPixShift = 20;
+
+template <int HW, int HH>
+__device__ __forceinline__ void census_pair(const uint8_t (*sL)[kCTX + 2 * kMaxHalf],
+                                            const uint8_t (*sR)[kCTX + 2 * kMaxHalf], int cx,
+                                            int cy, uint64_t& wl, uint64_t& wr) {
+  const uint8_t cl = sL[cy][cx], cr = sR[cy][cx];
+  uint32_t l0 = 0, l1 = 0, r0 = 0, r1 = 0;
+  int bit = 0;
+#pragma unroll
+  for (int dy = -HH; dy <= HH; ++dy)
+#pragma unroll
+    for (int dx = -HW; dx <= HW; ++dx) {
+      if (dx == 0 && dy == 0) continue;
+      const uint32_t bl = sL[cy + dy][cx + dx] < cl, br = sR[cy + dy][cx + dx] < cr;
+      if (bit < 32) { l0 |= bl << bit; r0 |= br << bit; }
+      else { l1 |= bl << (bit - 32); r1 |= br << (bit - 32); }
+      ++bit;
+    }
+  wl = (uint64_t(l1) << 32) | l0;
+  wr = (uint64_t(r1) << 32) | r0;
+}
+
+__device__ __forceinline__ void census_generic(const uint8_t (*sL)[kCTX + 2 * kMaxHalf],
+                                               const uint8_t (*sR)[kCTX + 2 * kMaxHalf],
+                                               int cx, int cy, int hw, int hh, uint64_t& wl,
+                                               uint64_t& wr) {
+  const uint8_t cl = sL[cy][cx], cr = sR[cy][cx];
+  wl = wr = 0;
+  int bit = 0;
+  for (int dy = -hh; dy <= hh; ++dy)
+    for (int dx = -hw; dx <= hw; ++dx) {
+      if (dx == 0 && dy == 0) continue;
+      wl |= uint64_t(sL[cy + dy][cx + dx] < cl) << bit;
+      wr |= uint64_t(sR[cy + dy][cx + dx] < cr) << bit;
+      ++bit;
+    }
+}
+
+template <int HW, int HH>   // HW = 0: runtime window
 __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
   __shared__ uint8_t sL[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
   __shared__ uint8_t sR[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
@@ -91,30 +138,22 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
   __syncthreads();
   const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
   if (x >= W || y >= H) return;
-  const int hw = cfg.hw, hh = cfg.hh;
+  const int hw = HW ? HW : cfg.hw, hh = HW ? HH : cfg.hh;
   const int cx = threadIdx.x + kMaxHalf, cy = threadIdx.y + kMaxHalf;
   uint64_t wl = 0, wr = 0;
   if (x >= hw && x < W - hw && y >= hh && y < H - hh) {
-    const uint8_t cl = sL[cy][cx], cr = sR[cy][cx];
-    int bit = 0;
-    for (int dy = -hh; dy <= hh; ++dy)
-      for (int dx = -hw; dx <= hw; ++dx) {
-        if (dx == 0 && dy == 0) continue;
-        wl |= uint64_t(sL[cy + dy][cx + dx] < cl) << bit;
-        wr |= uint64_t(sR[cy + dy][cx + dx] < cr) << bit;
-        ++bit;
-      }
+    if (HW) census_pair<HW, HH>(sL, sR, cx, cy, wl, wr);
+    else census_generic(sL, sR, cx, cy, hw, hh, wl, wr);
   }
-  const size_t i = size_t(y) * W + x;
   if (cfg.packed) {
-    wl |= uint64_t(sL[cy][cx]) << 56;
-    wr |= uint64_t(sR[cy][cx]) << 56;
+    wl |= (uint64_t(kGuard) | (uint64_t(sL[cy][cx]) << kPixShift)) << 32;
+    wr |= (uint64_t(sR[cy][cx]) << kPixShift) << 32;
   }
   P.cwL[size_t(y) * P.cpitch + P.lpad + x] = wl;
   P.cwR[size_t(y) * P.cpitch + x] = wr;
   const int c = sL[cy][cx];
   P.ax[size_t(y) * P.apitch + P.lpad + x] = x > 0 ? srf[abs(c - int(sL[cy][cx - 1]))] : srf[0];
-  P.ay[i] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
+  P.ay[size_t(y) * W + x] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
 }
 
 // ---------------------------------------------------------------------------------
@@ -129,14 +168,12 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
 // valid output (the vertical passes stay within a column and the top-2 masks
 // k > x - hw - dmin), so they are not computed exactly and not needed.
 // Score table: (h, m) -> Q14 score, h = Hamming distance, m = |L - R| clamped to
-// TS-1 (exact: the AD score saturates at ad_trunc < TS).  With TS = 16 the table is
-// stored as int32 in 8 interleaved copies (lane l reads copy l & 7), which spreads
-// the warp's data-dependent lookups over the shared-memory banks.
+// TS-1 (exact: the AD score saturates at ad_trunc < TS).  Stored m-major with 64
+// h-entries per row, so the many lookups that share the saturated m read adjacent
+// entries, not one bank.
 template <int TS, int CP>
 struct ScoreTable {
-  __host__ __device__ static constexpr size_t bytes() {
-    return CP == 2 ? size_t(96) * 4 : size_t(66) * TS * (TS == 16 ? 4 * CP : 2);
-  }
+  __host__ __device__ static constexpr size_t bytes() { return size_t(TS) * 64 * 2; }
 };
 
 template <bool PACKED, int TS, int CP>
@@ -145,24 +182,15 @@ __device__ __forceinline__ int32_t graded(uint64_t lw, uint64_t rw, const void* 
                                           int xr) {
   int h, ad;
   if (PACKED) {
-    const uint32_t lo = uint32_t(lw) ^ uint32_t(rw);
-    const uint32_t hi = uint32_t(lw >> 32) ^ uint32_t(rw >> 32);
-    h = __popc(lo) + __popc(hi & 0x00FFFFFFu);
-    ad = abs(int(uint32_t(lw >> 56)) - int(uint32_t(rw >> 56)));
+    const uint32_t lh = uint32_t(lw >> 32), rh = uint32_t(rw >> 32);
+    h = __popc(uint32_t(lw) ^ uint32_t(rw)) + __popc((lh ^ rh) & kCensusHiMask);
+    ad = abs((int32_t(lh) - int32_t(rh)) >> kPixShift);
   } else {
     h = __popcll(lw ^ rw);
     ad = abs(int(sLp[xl]) - int(sRp[xr]));
   }
-  if (TS == 16 && CP == 2) {           // v = (C1[h] + A1[m]) >> 10, two small tables
-    ad = min(ad, 15);
-    const int32_t* t = static_cast<const int32_t*>(tab);
-    return (t[h] + t[66 + ad]) >> 10;
-  }
-  if (TS == 16) {
-    ad = min(ad, 15);
-    return static_cast<const int32_t*>(tab)[(h * 16 + ad) * CP];
-  }
-  return static_cast<const int16_t*>(tab)[h * TS + ad];
+  if (TS == 16) ad = min(ad, 15);
+  return static_cast<const int16_t*>(tab)[ad * 64 + h];
 }
 
 // Bulk asynchronous copies (cp.async.bulk, the TMA engine's 1-D form) with
@@ -237,28 +265,15 @@ __global__ void __launch_bounds__(128, 4) k_rows(DevCfg cfg, Batch b) {
     for (int i = 0; i < 2 + NS; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (TS == 16 && CP == 2) {
-    int32_t* t32 = reinterpret_cast<int32_t*>(tabp);
-    for (int i = tid; i < 96; i += blockDim.x)
-      t32[i] = i < 66 ? int32_t(cfg.tbl[i]) * (1024 - cfg.wq)
-                      : (i < 82 ? int32_t(cfg.adt[i - 66]) * cfg.wq : 0);
-  } else if (TS == 16) {
-    int32_t* t32 = reinterpret_cast<int32_t*>(tabp);
-    for (int i = tid; i < 66 * 16 * CP; i += blockDim.x) {
-      const int e = i / CP, h = e >> 4, m = e & 15;
-      t32[i] = (int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10;
-    }
-  } else {
+  {
     int16_t* t16 = reinterpret_cast<int16_t*>(tabp);
-    for (int i = tid; i < 66 * TS; i += blockDim.x) {
-      const int h = i / TS, m = i % TS;
+    for (int i = tid; i < TS * 64; i += blockDim.x) {
+      const int m = i >> 6, h = i & 63;
       t16[i] = int16_t((int32_t(cfg.tbl[h]) * (1024 - cfg.wq) + int32_t(cfg.adt[m]) * cfg.wq) >> 10);
     }
   }
   __syncthreads();
-  const void* tab = (TS == 16 && CP != 2)
-                        ? static_cast<const void*>(reinterpret_cast<const int32_t*>(tabp) + (tid % CP))
-                        : static_cast<const void*>(tabp);
+  const void* tab = static_cast<const void*>(tabp);
   const int hw = cfg.hw, dmin = cfg.dmin;
   const int total = b.rows_prefix[b.n];
   int* err = b.err;
@@ -897,8 +912,7 @@ size_t rows_smem(const Batch& b, int TS, int CP, bool packed) {
     apm = std::max(apm, b.p[i].apitch);
     maxW = std::max(maxW, b.p[i].W);
   }
-  size_t tab = (TS == 16) ? (CP == 2 ? ScoreTable<16, 2>::bytes() : size_t(66) * 16 * 4 * CP)
-                          : ScoreTable<256, 1>::bytes();
+  size_t tab = (TS == 16) ? ScoreTable<16, 1>::bytes() : ScoreTable<256, 1>::bytes();
   size_t s = (tab + 127) & ~size_t(127);
   s += 2 * ((size_t(cpm) * 16 + size_t(apm) * 2 + 127) & ~size_t(127));
   s += size_t(b.bwd_stages) * b.bwd_chunk * b.maxDpad * 2;
@@ -909,8 +923,6 @@ size_t rows_smem(const Batch& b, int TS, int CP, bool packed) {
 struct de_cfg_hw { int hw, dmin; };
 int g_cols_stage_kb = 32;         // column kernel: shared bytes for the row ring
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
-int g_rows_table_copies = 2;      // score-table form: 1 = one 2D table, 8 = eight
-                                  // interleaved copies, 2 = split C1[h] + A1[m]
 
 size_t solve_smem(int W) { return size_t(W) * 53 + 64; }
 
@@ -924,7 +936,9 @@ cudaError_t set_smem(K kernel, size_t bytes) {
 cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int tiles = b.pix_prefix[b.n];
   if (tiles == 0) return cudaSuccess;
-  k_census<<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
+  if (cfg.hw == 3 && cfg.hh == 3) k_census<3, 3><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
+  else if (cfg.hw == 4 && cfg.hh == 3) k_census<4, 3><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
+  else k_census<0, 0><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
   return cudaGetLastError();
 }
 
@@ -949,24 +963,16 @@ cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int items = b.rows_prefix[b.n];
   if (items == 0) return cudaSuccess;
   const int TS = cfg.trunc < 16 ? 16 : 256;
-  const int CP = (TS == 16) ? g_rows_table_copies : 1;
+  const int CP = 1;
   const size_t sm = rows_smem(b, TS, CP, cfg.packed != 0);
   const int threads = b.maxDpad / 2;
   if (TS == 256)
     return cfg.packed ? launch_rows_t<true, 256, 1>(cfg, b, sm, threads, s)
                       : launch_rows_t<false, 256, 1>(cfg, b, sm, threads, s);
-  if (CP == 8)
-    return cfg.packed ? launch_rows_t<true, 16, 8>(cfg, b, sm, threads, s)
-                      : launch_rows_t<false, 16, 8>(cfg, b, sm, threads, s);
-  if (CP == 2)
-    return cfg.packed ? launch_rows_t<true, 16, 2>(cfg, b, sm, threads, s)
-                      : launch_rows_t<false, 16, 2>(cfg, b, sm, threads, s);
   return cfg.packed ? launch_rows_t<true, 16, 1>(cfg, b, sm, threads, s)
                     : launch_rows_t<false, 16, 1>(cfg, b, sm, threads, s);
 }
 
-void set_rows_table_copies(int v) { g_rows_table_copies = (v == 8 || v == 2) ? v : 1; }
-int get_rows_table_copies() { return g_rows_table_copies; }
 void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }
 int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
 

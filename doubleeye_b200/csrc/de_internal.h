@@ -91,8 +91,6 @@ int get_rows_ctas_per_sm();
 void set_cols_kt(int v);
 void set_cols_stage_kb(int v);
 int get_cols_stage_kb();
-void set_rows_table_copies(int v);
-int get_rows_table_copies();
 int get_cols_kt();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 

@@ -147,10 +147,6 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *   "rows_ctas_per_sm"  cap on row-kernel CTAs resident per SM (default 32, i.e.
  *                       as many as fit): fewer rows in flight keep each row's
  *                       forward pass in L2 for its backward pass
- *   "rows_table_copies" score-table form in shared memory: 1 = one (h, m) table,
- *                       8 = eight interleaved copies (spreads data-dependent
- *                       lookups over the banks), 2 = split census and AD tables
- *                       summed before the shift (default 2)
  *   "cols_kt"           disparities per lane in the column kernel: 8, 16, or 0 to
  *                       choose by batch size (default 0)
  *   "cols_stage_kb"     shared memory (KB) for the column kernel's row ring; its

@@ -236,33 +236,38 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async;" ::: "memory");
 }
 
-// One row per CTA iteration (the grid is persistent over rows).  The row's census
-// words and x-coefficients arrive by three bulk copies, double-buffered so the next
-// row's inputs load while this row computes.  The forward results go to the volume
-// with plain stores; the backward pass brings them back through a ring of bulk
-// copies (bwd_chunk columns each, bwd_stages deep), so no thread waits on a
-// global load.
-template <bool PACKED, int TS, int CP>
-__global__ void __launch_bounds__(128, 4) k_rows(DevCfg cfg, Batch b) {
+// One row per CTA iteration (the grid is persistent over rows); all pairs of a
+// launch share Dpad = 64 G, so strides and chunk sizes are compile-time.  The row's
+// census words arrive by bulk copy into a single buffer that is refilled for the
+// next row while this row's backward pass runs (only the forward pass reads them);
+// the x-coefficients, read by both passes, are double-buffered.  Forward results go
+// to the volume with plain stores; the backward pass brings them back through a
+// ring of bulk copies, so no thread waits on a global load.
+template <bool PACKED, int TS, int G>
+__global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
+  constexpr int DP = 64 * G;                          // Dpad
+  constexpr int XS = DP / 2;                          // x stride in 32-bit words
+  constexpr int CH = 2048 / DP;                       // x columns per backward chunk
+  constexpr int NS = 3;                               // backward ring depth
+  constexpr size_t STAGE = size_t(CH) * DP * 2;
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bars[2 + kMaxStages];
+  __shared__ __align__(8) uint64_t bars[4 + NS];      // census, ax[2], spare, ring
   int cpm = 0, apm = 0, maxW = 0;
   for (int i = 0; i < b.n; ++i) {
     cpm = max(cpm, b.p[i].cpitch);
     apm = max(apm, b.p[i].apitch);
     maxW = max(maxW, b.p[i].W);
   }
-  const int CH = b.bwd_chunk, NS = b.bwd_stages, maxDpad = b.maxDpad;
   uint8_t* tabp = smem;
-  uint8_t* inbuf = tabp + ((ScoreTable<TS, CP>::bytes() + 127) & ~size_t(127));
-  const size_t in_bytes = (size_t(cpm) * 16 + size_t(apm) * 2 + 127) & ~size_t(127);
-  uint8_t* bwdbuf = inbuf + 2 * in_bytes;
-  const size_t stage_bytes = size_t(CH) * maxDpad * 2;
-  uint8_t* sLp = bwdbuf + NS * stage_bytes;
+  uint8_t* cbuf = tabp + ScoreTable<TS, 1>::bytes();                 // L | R words
+  uint8_t* abuf = cbuf + size_t(cpm) * 16;                            // ax x 2
+  const size_t abytes = (size_t(apm) * 2 + 127) & ~size_t(127);
+  uint8_t* ring = abuf + 2 * abytes;
+  uint8_t* sLp = ring + NS * STAGE;
   uint8_t* sRp = sLp + maxW;
   const int tid = threadIdx.x;
   if (tid == 0) {
-    for (int i = 0; i < 2 + NS; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < 4 + NS; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   {
@@ -277,142 +282,169 @@ __global__ void __launch_bounds__(128, 4) k_rows(DevCfg cfg, Batch b) {
   const int hw = cfg.hw, dmin = cfg.dmin;
   const int total = b.rows_prefix[b.n];
   int* err = b.err;
+  const uint64_t* sL = reinterpret_cast<const uint64_t*>(cbuf);       // + lpad below
+  const uint64_t* sR = reinterpret_cast<const uint64_t*>(cbuf + size_t(cpm) * 8);
 
-  // row inputs of `item` into input buffer `buf` (thread 0 only)
-  auto issue_inputs = [&](int item, int buf) {
+  auto row_of = [&](int item, int* y) -> const DevPair& {
     const int pi = find_pair(b.rows_prefix, b.n, item);
-    const DevPair& P = b.p[pi];
-    const int y = cfg.hh + (item - b.rows_prefix[pi]);
-    uint8_t* dst = inbuf + buf * in_bytes;
-    const uint32_t cb = uint32_t(P.cpitch) * 8, ab = uint32_t(P.apitch) * 2;
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // buffer reads done
-    mbar_expect(&bars[buf], 2 * cb + ab);
-    bulk_load(dst, P.cwL + size_t(y) * P.cpitch, cb, &bars[buf]);
-    bulk_load(dst + size_t(cpm) * 8, P.cwR + size_t(y) * P.cpitch, cb, &bars[buf]);
-    bulk_load(dst + size_t(cpm) * 16, P.ax + size_t(y) * P.apitch, ab, &bars[buf]);
+    *y = cfg.hh + (item - b.rows_prefix[pi]);
+    return b.p[pi];
+  };
+  auto issue_census = [&](int item) {                 // thread 0
+    int y;
+    const DevPair& P = row_of(item, &y);
+    const uint32_t cb = uint32_t(P.cpitch) * 8;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(&bars[0], 2 * cb);
+    bulk_load(cbuf, P.cwL + size_t(y) * P.cpitch, cb, &bars[0]);
+    bulk_load(cbuf + size_t(cpm) * 8, P.cwR + size_t(y) * P.cpitch, cb, &bars[0]);
+  };
+  auto issue_ax = [&](int item, int buf) {            // thread 0
+    int y;
+    const DevPair& P = row_of(item, &y);
+    const uint32_t ab = uint32_t(P.apitch) * 2;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect(&bars[1 + buf], ab);
+    bulk_load(abuf + buf * abytes, P.ax + size_t(y) * P.apitch, ab, &bars[1 + buf]);
   };
 
   uint32_t phase = 0;                                 // parity bit per barrier
-  if (tid == 0 && int(blockIdx.x) < total) issue_inputs(blockIdx.x, 0);
+  auto wait_bar = [&](int i) {
+    mbar_wait(&bars[i], (phase >> i) & 1u, err);
+    phase ^= 1u << i;
+  };
+  if (tid == 0 && int(blockIdx.x) < total) { issue_census(blockIdx.x); issue_ax(blockIdx.x, 0); }
   int it = 0;
   for (int item = blockIdx.x; item < total; item += gridDim.x, ++it) {
     const int buf = it & 1;
-    if (tid == 0 && item + int(gridDim.x) < total) issue_inputs(item + gridDim.x, buf ^ 1);
-    const int pi = find_pair(b.rows_prefix, b.n, item);
-    const DevPair& P = b.p[pi];
-    const int W = P.W, Dpad = P.Dpad;
-    const int y = cfg.hh + (item - b.rows_prefix[pi]);
+    const int next = item + int(gridDim.x);
+    if (tid == 0 && next < total) issue_ax(next, buf ^ 1);
+    int y;
+    const DevPair& P = row_of(item, &y);
+    const int W = P.W;
     const size_t row = size_t(y) * W;
-    mbar_wait(&bars[buf], (phase >> buf) & 1u, err);
-    phase ^= 1u << buf;
-    const uint8_t* ib = inbuf + buf * in_bytes;
-    const uint64_t* sL = reinterpret_cast<const uint64_t*>(ib) + P.lpad;
-    const uint64_t* sR = reinterpret_cast<const uint64_t*>(ib + size_t(cpm) * 8);
-    const uint16_t* sax = reinterpret_cast<const uint16_t*>(ib + size_t(cpm) * 16) + P.lpad;
+    wait_bar(0);
+    wait_bar(1 + buf);
+    const uint64_t* sLx = sL + P.lpad;
+    const uint16_t* sax = reinterpret_cast<const uint16_t*>(abuf + buf * abytes) + P.lpad;
     if (!PACKED) {
       for (int i = tid; i < W; i += blockDim.x) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
       __syncthreads();
     }
-    const bool active = 2 * tid < Dpad;
     const int d0 = dmin + 2 * tid;
     const int xw = hw + dmin + 2 * (tid & ~31);       // first lane's start in this warp
     const int xend = W - hw;                          // scores are 0 from here on
-    uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * Dpad) + tid;
-    const size_t xs = size_t(Dpad) >> 1;              // x stride in 32-bit words
+    uint32_t* out = reinterpret_cast<uint32_t*>(P.vol + row * DP) + tid;
     int32_t f0 = 0, f1 = 0;
-    if (active) {
-      uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;  // chain k1's word
+    {
+      uint64_t rprev = (xw - 1 - d0 >= 0) ? sR[xw - 1 - d0] : 0;    // chain k1's word
       int x = xw;
       int xramp = min(xend, xw + 64);                 // lanes may still be before their start
       xramp += (xramp - dmin) & 1;                    // the paired loop needs x - dmin even
       xramp = min(xramp, xend);
       for (; x < xramp; ++x) {
         const int32_t a = sax[x];
-        const uint64_t lw = sL[x];
+        const uint64_t lw = sLx[x];
         int32_t v0 = 0, v1 = 0;
         uint64_t rw = 0;
         if (x - d0 >= hw) {
           rw = sR[x - d0];
-          v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
+          v0 = graded<PACKED, TS, 1>(lw, rw, tab, sLp, sRp, x, x - d0);
         }
-        if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
+        if (x - d0 - 1 >= hw) v1 = graded<PACKED, TS, 1>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
         rprev = rw;
         f0 = rf_step(v0, f0, a);
         f1 = rf_step(v1, f1, a);
-        out[x * xs] = pack2(f0, f1);
+        out[x * XS] = pack2(f0, f1);
       }
+      const uint64_t* rp = sR + (x - d0);
+      const uint64_t* lp = sLx + x;
+      const uint16_t* ap = sax + x;
+      uint32_t* op = out + x * XS;
 #pragma unroll 2
       for (; x + 1 < xend; x += 2) {                  // two x per iteration
-        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(sax + x);
-        const ulonglong2 l2 = *reinterpret_cast<const ulonglong2*>(sL + x);
-        const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(sR + (x - d0));
+        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(ap);
+        const ulonglong2 l2 = *reinterpret_cast<const ulonglong2*>(lp);
+        const ulonglong2 r2 = *reinterpret_cast<const ulonglong2*>(rp);
         const int32_t a0 = int32_t(a2 & 0xFFFFu), a1 = int32_t(a2 >> 16);
-        const int32_t v00 = graded<PACKED, TS, CP>(l2.x, r2.x, tab, sLp, sRp, x, x - d0);
-        const int32_t v01 = graded<PACKED, TS, CP>(l2.x, rprev, tab, sLp, sRp, x, x - d0 - 1);
-        const int32_t v10 = graded<PACKED, TS, CP>(l2.y, r2.y, tab, sLp, sRp, x + 1, x + 1 - d0);
-        const int32_t v11 = graded<PACKED, TS, CP>(l2.y, r2.x, tab, sLp, sRp, x + 1, x - d0);
+        const int32_t v00 = graded<PACKED, TS, 1>(l2.x, r2.x, tab, sLp, sRp, x, x - d0);
+        const int32_t v01 = graded<PACKED, TS, 1>(l2.x, rprev, tab, sLp, sRp, x, x - d0 - 1);
+        const int32_t v10 = graded<PACKED, TS, 1>(l2.y, r2.y, tab, sLp, sRp, x + 1, x + 1 - d0);
+        const int32_t v11 = graded<PACKED, TS, 1>(l2.y, r2.x, tab, sLp, sRp, x + 1, x - d0);
         rprev = r2.y;
         f0 = rf_step(v00, f0, a0);
         f1 = rf_step(v01, f1, a0);
-        out[x * xs] = pack2(f0, f1);
+        op[0] = pack2(f0, f1);
         f0 = rf_step(v10, f0, a1);
         f1 = rf_step(v11, f1, a1);
-        out[(x + 1) * xs] = pack2(f0, f1);
+        op[XS] = pack2(f0, f1);
+        rp += 2; lp += 2; ap += 2; op += 2 * XS;
       }
       for (; x < xend; ++x) {                         // at most one leftover step
         const int32_t a = sax[x];
-        const uint64_t lw = sL[x];
+        const uint64_t lw = sLx[x];
         const uint64_t rw = sR[x - d0];
-        const int32_t v0 = graded<PACKED, TS, CP>(lw, rw, tab, sLp, sRp, x, x - d0);
-        const int32_t v1 = graded<PACKED, TS, CP>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
+        const int32_t v0 = graded<PACKED, TS, 1>(lw, rw, tab, sLp, sRp, x, x - d0);
+        const int32_t v1 = graded<PACKED, TS, 1>(lw, rprev, tab, sLp, sRp, x, x - d0 - 1);
         rprev = rw;
         f0 = rf_step(v0, f0, a);
         f1 = rf_step(v1, f1, a);
-        out[x * xs] = pack2(f0, f1);
+        out[x * XS] = pack2(f0, f1);
       }
       for (; x < W; ++x) {                            // right border, score 0
         const int32_t a = sax[x];
         f0 = rf_step(0, f0, a);
         f1 = rf_step(0, f1, a);
-        out[x * xs] = pack2(f0, f1);
+        out[x * XS] = pack2(f0, f1);
       }
     }
-    // backward: forward results come back by bulk copy, chunk by chunk from the right
+    // backward; the census buffer is free now, so the next row's words start loading
     fence_proxy_async();                              // our stores before the async reads
     __syncthreads();
+    if (tid == 0 && next < total) issue_census(next);
     const int xlo_cta = hw + dmin;
     const int jmax = (W - 2) / CH, jmin = xlo_cta / CH;
     auto issue_chunk = [&](int j, int slot) {
       const int xa = j * CH;
-      const uint32_t bytes = uint32_t(min(CH, W - xa)) * uint32_t(Dpad) * 2u;
+      const uint32_t bytes = uint32_t(min(CH, W - xa)) * uint32_t(DP) * 2u;
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // stage reads done
-      mbar_expect(&bars[2 + slot], bytes);
-      bulk_load(bwdbuf + slot * stage_bytes, P.vol + (row + xa) * Dpad, bytes, &bars[2 + slot]);
+      mbar_expect(&bars[4 + slot], bytes);
+      bulk_load(ring + slot * STAGE, P.vol + (row + xa) * DP, bytes, &bars[4 + slot]);
     };
     if (tid == 0)
       for (int q = 0; q < NS && jmax - q >= jmin; ++q) issue_chunk(jmax - q, q);
     int32_t g0 = f0, g1 = f1;                         // seed: forward value at W-1
     int slot = 0;
     for (int j = jmax; j >= jmin; --j) {
-      mbar_wait(&bars[2 + slot], (phase >> (2 + slot)) & 1u, err);
-      phase ^= 1u << (2 + slot);
-      if (active) {
-        const int xa = j * CH;
-        const uint32_t* cb = reinterpret_cast<const uint32_t*>(bwdbuf + slot * stage_bytes) + tid;
-        const int xlo = max(xa, xw);
-        for (int x = min(W - 2, xa + CH - 1); x >= xlo; --x) {
-          const uint32_t c = cb[(x - xa) * xs];
+      wait_bar(4 + slot);
+      const int xa = j * CH;
+      const uint32_t* cb = reinterpret_cast<const uint32_t*>(ring + slot * STAGE) + tid;
+      const int xhi = min(W - 2, xa + CH - 1);
+      const int xlo = max(xa, xw);
+      if (xhi == xa + CH - 1 && xlo == xa) {          // a full chunk: unrolled
+        uint32_t* o = out + xa * XS;
+        const uint16_t* a1p = sax + xa + 1;
+#pragma unroll
+        for (int q = CH - 1; q >= 0; --q) {
+          const uint32_t c = cb[q * XS];
+          const int32_t a = a1p[q];
+          g0 = rf_step(lo16(c), g0, a);
+          g1 = rf_step(hi16(c), g1, a);
+          o[q * XS] = pack2(g0, g1);
+        }
+      } else {
+        for (int x = xhi; x >= xlo; --x) {
+          const uint32_t c = cb[(x - xa) * XS];
           const int32_t a = sax[x + 1];
           g0 = rf_step(lo16(c), g0, a);
           g1 = rf_step(hi16(c), g1, a);
-          out[x * xs] = pack2(g0, g1);
+          out[x * XS] = pack2(g0, g1);
         }
       }
       __syncthreads();                                // stage consumed by every thread
       if (tid == 0 && j - NS >= jmin) issue_chunk(j - NS, slot);
       slot = (slot + 1 == NS) ? 0 : slot + 1;
     }
-    __syncthreads();                                  // input buffer free for reuse
   }
 }
 
@@ -905,24 +937,20 @@ __global__ void k_export(DevCfg cfg, Batch b) {
   }
 }
 
-size_t rows_smem(const Batch& b, int TS, int CP, bool packed) {
+size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   int cpm = 0, apm = 0, maxW = 0;
   for (int i = 0; i < b.n; ++i) {
     cpm = std::max(cpm, b.p[i].cpitch);
     apm = std::max(apm, b.p[i].apitch);
     maxW = std::max(maxW, b.p[i].W);
   }
-  size_t tab = (TS == 16) ? ScoreTable<16, 1>::bytes() : ScoreTable<256, 1>::bytes();
-  size_t s = (tab + 127) & ~size_t(127);
-  s += 2 * ((size_t(cpm) * 16 + size_t(apm) * 2 + 127) & ~size_t(127));
-  s += size_t(b.bwd_stages) * b.bwd_chunk * b.maxDpad * 2;
+  size_t s = size_t(TS) * 64 * 2;
+  s += size_t(cpm) * 16;
+  s += 2 * ((size_t(apm) * 2 + 127) & ~size_t(127));
+  s += size_t(3) * (2048 / (64 * G)) * (64 * G) * 2;
   if (!packed) s += size_t(maxW) * 2;
   return (s + 15) & ~size_t(15);
 }
-
-struct de_cfg_hw { int hw, dmin; };
-int g_cols_stage_kb = 32;         // column kernel: shared bytes for the row ring
-int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
 
 size_t solve_smem(int W) { return size_t(W) * 53 + 64; }
 
@@ -942,35 +970,61 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template <bool PACKED, int TS, int CP>
-cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, size_t sm, int threads,
-                          cudaStream_t s) {
-  cudaError_t e = set_smem(k_rows<PACKED, TS, CP>, sm);
+struct de_cfg_hw { int hw, dmin; };
+int g_cols_stage_kb = 32;         // column kernel: shared bytes for the row ring
+int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
+
+template <bool PACKED, int TS, int G>
+cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  const size_t sm = rows_smem(b, TS, G, PACKED);
+  cudaError_t e = set_smem(k_rows<PACKED, TS, G>, sm);
   if (e != cudaSuccess) return e;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   int fit = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_rows<PACKED, TS, CP>, threads, sm);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_rows<PACKED, TS, G>, 32 * G, sm);
   const int per_sm = std::max(1, std::min(fit > 0 ? fit : 1, g_rows_ctas_per_sm));
   const int items = b.rows_prefix[b.n];
   const int grid = std::min(items, per_sm * nsm);
-  k_rows<PACKED, TS, CP><<<grid, threads, sm, s>>>(cfg, b);
+  k_rows<PACKED, TS, G><<<grid, 32 * G, sm, s>>>(cfg, b);
   return cudaGetLastError();
 }
 
-cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
-  const int items = b.rows_prefix[b.n];
-  if (items == 0) return cudaSuccess;
+template <int G>
+cudaError_t launch_rows_g(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int TS = cfg.trunc < 16 ? 16 : 256;
-  const int CP = 1;
-  const size_t sm = rows_smem(b, TS, CP, cfg.packed != 0);
-  const int threads = b.maxDpad / 2;
-  if (TS == 256)
-    return cfg.packed ? launch_rows_t<true, 256, 1>(cfg, b, sm, threads, s)
-                      : launch_rows_t<false, 256, 1>(cfg, b, sm, threads, s);
-  return cfg.packed ? launch_rows_t<true, 16, 1>(cfg, b, sm, threads, s)
-                    : launch_rows_t<false, 16, 1>(cfg, b, sm, threads, s);
+  if (cfg.packed)
+    return TS == 16 ? launch_rows_t<true, 16, G>(cfg, b, s) : launch_rows_t<true, 256, G>(cfg, b, s);
+  return TS == 16 ? launch_rows_t<false, 16, G>(cfg, b, s) : launch_rows_t<false, 256, G>(cfg, b, s);
+}
+
+// One launch per disparity group present in the batch (Dpad = 64 G).
+cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  if (b.rows_prefix[b.n] == 0) return cudaSuccess;
+  thread_local Batch sub;
+  for (int G = 1; G <= 4; ++G) {
+    sub = b;
+    sub.n = 0;
+    sub.rows_prefix[0] = 0;
+    sub.maxDpad = 64 * G;
+    for (int i = 0; i < b.n; ++i) {
+      if (b.p[i].Dpad != 64 * G) continue;
+      sub.p[sub.n] = b.p[i];
+      sub.rows_prefix[sub.n + 1] = sub.rows_prefix[sub.n] + (b.rows_prefix[i + 1] - b.rows_prefix[i]);
+      ++sub.n;
+    }
+    if (sub.n == 0 || sub.rows_prefix[sub.n] == 0) continue;
+    cudaError_t e;
+    switch (G) {
+      case 1: e = launch_rows_g<1>(cfg, sub, s); break;
+      case 2: e = launch_rows_g<2>(cfg, sub, s); break;
+      case 3: e = launch_rows_g<3>(cfg, sub, s); break;
+      default: e = launch_rows_g<4>(cfg, sub, s); break;
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }

@@ -85,6 +85,7 @@ SIGNATURES = {
                                            C.POINTER(C.c_size_t)]),
     "de_dense_dev": (C.c_int, [C.POINTER(DeCfg), C.POINTER(DePair), C.c_int, vp, C.c_size_t,
                                vp]),
+    "de_dense_noalloc_dev": (C.c_int, [C.POINTER(DeCfg), C.POINTER(DePair), vp]),
     "de_census_dev": (C.c_int, [C.POINTER(DeCfg), vp, vp, C.c_int, C.c_int, vp, vp, vp, vp,
                                 vp]),
     "de_cost_workspace_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),

@@ -70,6 +70,14 @@ int check_dims(int W, int H) {
 
 namespace de {
 
+int set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
 // Host-built tables, the same expressions as the reference so the values agree bit
 // for bit: the filter LUT core/tools/de_dense.cpp:533-546 (float, std::exp), the
 // score tables :1201-1223.

@@ -73,6 +73,9 @@ struct Batch {
   DevPair p[kMaxBatch];
 };
 
+// Records a one-line reason for de_last_error() and returns code (de_capi.cu).
+int set_error(int code, const char* fmt, ...);
+
 // Host-side preparation (de_capi.cu).
 void make_dev_cfg(const de_cfg& c, DevCfg* out);
 size_t pair_workspace_bytes(int W, int H, int D, bool lrc);

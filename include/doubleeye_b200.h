@@ -108,6 +108,18 @@ DE_API int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int
 DE_API int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n,
                         void* workspace, size_t ws_bytes, void* stream);
 
+/* The same dense pipeline for one pair with NO allocation anywhere: for callers
+ * that cannot call cudaMalloc (inside a graph capture that must not allocate, on
+ * real-time threads, under a host that owns the device heap).  No counterpart in
+ * the reference.  The workspace is a 16 MiB file-scope device array that every GPU
+ * loading this library holds until exit; a pair whose de_dense_workspace_bytes
+ * exceeds it is refused with DE_ERR_ARG (the default 7x7 census fits 320x240 at
+ * D <= 64).  The first call on a device resolves the array's device address with
+ * that device current, so make that first call before any stream capture.  Calls
+ * share the array: calls whose work overlaps on the GPU (concurrent streams,
+ * devices aside) race and must be serialised by the caller. */
+DE_API int de_dense_noalloc_dev(const de_cfg* cfg, const de_pair* pair, void* stream);
+
 /* Status of the last launch set that used this workspace: waits for the stream,
  * then writes 0, or non-zero if a bounded device wait ran out (the results of that
  * launch set are then invalid).  The host-pointer context checks it itself. */

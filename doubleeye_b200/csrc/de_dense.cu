@@ -706,20 +706,25 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   const int y = item - b.solve_prefix[pi];
   const int dmin = cfg.dmin, hw = cfg.hw, hh = cfg.hh;
   const float lambda = cfg.lambda, gamma = cfg.gamma, damping = cfg.damping, keep = cfg.keep;
-  float* s_cs = reinterpret_cast<float*>(smem);          // [2W]
+  // shared layout (bytes per pixel): cs 8, beta 8, rho 8, margin 4, best 4, start 4,
+  // cur 4, items 4, lo 4, hi 4, cd 2, rev 2, cn 1, bestj 1, win 1  = 59
+  float* s_cs = reinterpret_cast<float*>(smem);          // [2W] item = 2x + j
   float* s_beta = s_cs + 2 * W;                           // [2W]
   float* s_rho = s_beta + 2 * W;                          // [2W]
-  float* s_best = s_rho + 2 * W;                          // [W]
-  float* s_margin = s_best + W;                           // [W]
-  int* s_start = reinterpret_cast<int*>(s_margin + W);    // [W+1]
+  float* s_margin = s_rho + 2 * W;                        // [W]
+  float* s_best = s_margin + W;                           // [W]
+  int* s_start = reinterpret_cast<int*>(s_best + W);      // [W+1]
   int* s_cur = s_start + W + 1;                           // [W]
-  int16_t* s_items = reinterpret_cast<int16_t*>(s_cur + W);   // [2W]
-  int16_t* s_cd = s_items + 2 * W;                        // [2W]
-  int16_t* s_rev = s_cd + 2 * W;                          // [W]
+  int16_t* s_items = reinterpret_cast<int16_t*>(s_cur + W);   // [2W] sorted by bucket
+  int16_t* s_lo = s_items + 2 * W;                        // [2W] bucket bounds of a position
+  int16_t* s_hi = s_lo + 2 * W;                           // [2W]
+  uint8_t* s_cd = reinterpret_cast<uint8_t*>(s_hi + 2 * W);  // [2W] k (valid for j < cn)
+  int16_t* s_rev = reinterpret_cast<int16_t*>(s_cd + 2 * W + (W & 1) * 2);  // [W]
   int8_t* s_cn = reinterpret_cast<int8_t*>(s_rev + W);    // [W]
   int8_t* s_bestj = s_cn + W;                             // [W]
   uint8_t* s_win = reinterpret_cast<uint8_t*>(s_bestj + W);  // [W]
   __shared__ int warp_sums[kSolveThreads / 32];
+  __shared__ int s_nitems;
   const int tid = threadIdx.x;
   const bool row_ok = y >= hh && y < H - hh;
   const size_t row = size_t(y) * W;
@@ -729,7 +734,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   for (int x = tid; x < W; x += kSolveThreads) {
     int n = 0;
     float c0 = kNegBig, c1 = kNegBig;
-    int k0 = -1, k1 = -1;
+    int k0 = 0, k1 = 0;
     if (REF_LAYOUT) {
       n = P.ref_cn[row + x];
       if (n > 0) { c0 = P.ref_cs[2 * (row + x)]; k0 = P.ref_cd[2 * (row + x)]; }
@@ -739,36 +744,46 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       if (a) { c0 = float(int32_t(a >> 8) - 32768) * q; k0 = 255 - int(a & 255u); n = 1; }
       if (bb) { c1 = float(int32_t(bb >> 8) - 32768) * q; k1 = 255 - int(bb & 255u); n = 2; }
     }
-    s_cs[2 * x] = c0; s_cs[2 * x + 1] = c1;
-    s_cd[2 * x] = int16_t(k0); s_cd[2 * x + 1] = int16_t(k1);
+    reinterpret_cast<float2*>(s_cs)[x] = make_float2(c0, c1);
+    s_cd[2 * x] = uint8_t(k0);
+    s_cd[2 * x + 1] = uint8_t(k1);
     s_cn[x] = int8_t(n);
     const float alt = (n < 2) ? lambda : fmax_ref(c1, lambda);
     const float m = (n == 0) ? 0.f : c0 - alt;
     s_margin[x] = m;
     if (P.margin) P.margin[row + x] = m;
     s_start[x] = 0;
-    s_beta[2 * x] = s_beta[2 * x + 1] = 0.f;
-    s_rho[2 * x] = s_rho[2 * x + 1] = 0.f;
+    reinterpret_cast<float2*>(s_beta)[x] = make_float2(0.f, 0.f);
+    reinterpret_cast<float2*>(s_rho)[x] = make_float2(0.f, 0.f);
     s_win[x] = 0;
   }
+  if (tid == 0) s_start[W] = 0;
   __syncthreads();
-  // 2. claimant buckets by right pixel (:270-284); order inside a bucket is free
+  // 2. claimant buckets by right pixel, counting sort (:270-284); order inside a
+  //    bucket is free: only its maxima are ever read
   for (int x = tid; x < W; x += kSolveThreads)
     for (int j = 0; j < s_cn[x]; ++j) {
       const int xr = x - (dmin + s_cd[2 * x + j]);
-      if (xr >= 0 && xr < W) atomicAdd(&s_start[xr], 1);
+      if (xr >= 0) atomicAdd(&s_start[xr], 1);
     }
   __syncthreads();
   block_excl_scan(s_start, W, warp_sums);
   for (int xr = tid; xr < W; xr += kSolveThreads) s_cur[xr] = s_start[xr];
+  if (tid == 0) s_nitems = s_start[W];
   __syncthreads();
   for (int x = tid; x < W; x += kSolveThreads)
     for (int j = 0; j < s_cn[x]; ++j) {
       const int xr = x - (dmin + s_cd[2 * x + j]);
-      if (xr >= 0 && xr < W) s_items[atomicAdd(&s_cur[xr], 1)] = int16_t(2 * x + j);
+      if (xr >= 0) {
+        const int p = atomicAdd(&s_cur[xr], 1);
+        s_items[p] = int16_t(2 * x + j);
+        s_lo[p] = int16_t(s_start[xr]);
+        s_hi[p] = int16_t(s_start[xr + 1]);
+      }
     }
   __syncthreads();
-  // 3. reverse match over surviving candidates (:303-313): first maximum in x order
+  const int nitems = s_nitems;
+  // 3. reverse match over the surviving candidates (:303-313): first maximum in x order
   for (int xr = tid; xr < W; xr += kSolveThreads) {
     int bd = -1, bi = 1 << 30;
     float bv = kNegBig;
@@ -779,49 +794,46 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     }
     s_rev[xr] = int16_t(bd);
   }
-  // 4. damped max-sum iterations (:318-341)
+  // 4. damped max-sum iterations (:318-341).  rho per pixel; beta per bucket member,
+  //    "max over the bucket excluding me" read directly from the other members.
   for (int it = 0; it < cfg.iters; ++it) {
     __syncthreads();
     for (int x = tid; x < W; x += kSolveThreads) {
       const int n = s_cn[x];
-      for (int j = 0; j < n; ++j) {
-        const float ex = (n == 2) ? s_beta[2 * x + 1 - j] : kNegBig;
-        const float tgt = s_cs[2 * x + j] - fmax_ref(lambda, ex);
-        s_rho[2 * x + j] = keep * tgt + damping * s_rho[2 * x + j];
-      }
+      if (n == 0) continue;
+      const float2 cs2 = reinterpret_cast<const float2*>(s_cs)[x];
+      const float2 be = reinterpret_cast<const float2*>(s_beta)[x];
+      float2 rh = reinterpret_cast<const float2*>(s_rho)[x];
+      const float ex0 = (n == 2) ? be.y : kNegBig;
+      rh.x = keep * (cs2.x - fmax_ref(lambda, ex0)) + damping * rh.x;
+      if (n == 2) rh.y = keep * (cs2.y - fmax_ref(lambda, be.x)) + damping * rh.y;
+      reinterpret_cast<float2*>(s_rho)[x] = rh;
     }
     __syncthreads();
-    for (int xr = tid; xr < W; xr += kSolveThreads) {
-      const int lo = s_start[xr], hi = s_start[xr + 1];
-      if (hi <= lo) continue;
-      float b1 = kNegBig, b2 = kNegBig;
-      int i1 = -1;
-      for (int p = lo; p < hi; ++p) {
-        const float v = s_rho[s_items[p]];
-        if (v > b1) { b2 = b1; b1 = v; i1 = p; } else if (v > b2) { b2 = v; }
-      }
-      for (int p = lo; p < hi; ++p) {
-        const int idx = s_items[p];
-        const float ex = (p == i1) ? b2 : b1;
-        s_beta[idx] = keep * (s_cs[idx] - fmax_ref(gamma, ex)) + damping * s_beta[idx];
-      }
+    for (int p = tid; p < nitems; p += kSolveThreads) {
+      const int idx = s_items[p];
+      const int lo = s_lo[p], hi = s_hi[p];
+      float ex = kNegBig;
+      for (int r = lo; r < hi; ++r)
+        if (r != p) ex = fmax_ref(ex, s_rho[s_items[r]]);
+      s_beta[idx] = keep * (s_cs[idx] - fmax_ref(gamma, ex)) + damping * s_beta[idx];
     }
   }
   __syncthreads();
-  // 5. belief (:343-358)
+  // 5. belief (:343-358) and the gates (:364-374) folded into eligibility
   for (int x = tid; x < W; x += kSolveThreads) {
     float best = kNegBig;
     int bj = -1;
-    for (int j = 0; j < s_cn[x]; ++j) {
+    const int n = s_cn[x];
+    for (int j = 0; j < n; ++j) {
       const float c = s_cs[2 * x + j];
       if (c <= lambda) continue;
       const float bel = (cfg.iters > 0) ? (s_beta[2 * x + j] + s_rho[2 * x + j] - c) : c;
       if (bel > best) { best = bel; bj = j; }
     }
-    // gates (:364-374) fold into eligibility
     if (bj >= 0 && cfg.min_margin > 0.f && s_margin[x] < cfg.min_margin) bj = -1;
     if (bj >= 0 && cfg.min_ratio > 0.f) {
-      const float s2 = (s_cn[x] > 1) ? fmax_ref(s_cs[2 * x + 1], lambda) : lambda;
+      const float s2 = (n > 1) ? fmax_ref(s_cs[2 * x + 1], lambda) : lambda;
       const float c1 = fmax_ref(1.f - s_cs[2 * x], 1e-6f);
       if ((1.f - s2) / c1 < cfg.min_ratio) bj = -1;
     }
@@ -851,6 +863,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   for (int x = tid; x < W; x += kSolveThreads) {
     float dl = __int_as_float(0x7fc00000);
     const int n = s_cn[x];
+    const float2 cs2 = reinterpret_cast<const float2*>(s_cs)[x];
     if (s_win[x]) {
       const int j = s_bestj[x];
       const int d = dmin + s_cd[2 * x + j];
@@ -863,7 +876,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
           const uint32_t nb = P.nb[row + x];
           m16 = lo16(nb); p16 = hi16(nb);
         }
-        const float c0 = s_cs[2 * x];
+        const float c0 = cs2.x;
         const float cm = (m16 == -32768) ? kNegBig : float(m16) * q;
         const float cp = (p16 == -32768) ? kNegBig : float(p16) * q;
         if (cm > -1e29f && cp > -1e29f) {
@@ -893,8 +906,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       }
     }
     if (P.lrc2) P.lrc2[row + x] = lrc2;
-    const float s1 = n > 0 ? s_cs[2 * x] : kNegBig;
-    const float s2 = n > 1 ? s_cs[2 * x + 1] : kNegBig;
+    const float s1 = n > 0 ? cs2.x : kNegBig;
+    const float s2 = n > 1 ? cs2.y : kNegBig;
     if (P.cand) {
       P.cand[row + x] = s1;
       P.cand[WH + row + x] = s2;
@@ -952,7 +965,7 @@ size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   return (s + 15) & ~size_t(15);
 }
 
-size_t solve_smem(int W) { return size_t(W) * 53 + 64; }
+size_t solve_smem(int W) { return size_t(W) * 59 + 64; }
 
 template <typename K>
 cudaError_t set_smem(K kernel, size_t bytes) {

@@ -458,6 +458,7 @@ int de_set_param(const char* name, int value) {
   if (!std::strcmp(name, "rows_ctas_per_sm")) { de::set_rows_ctas_per_sm(value); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { de::set_cols_kt(value); return DE_OK; }
   if (!std::strcmp(name, "cols_stage_kb")) { de::set_cols_stage_kb(value); return DE_OK; }
+  if (!std::strcmp(name, "solve_threads")) { de::set_solve_threads(value); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 
@@ -466,6 +467,7 @@ int de_get_param(const char* name, int* value) {
   if (!std::strcmp(name, "rows_ctas_per_sm")) { *value = de::get_rows_ctas_per_sm(); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { *value = de::get_cols_kt(); return DE_OK; }
   if (!std::strcmp(name, "cols_stage_kb")) { *value = de::get_cols_stage_kb(); return DE_OK; }
+  if (!std::strcmp(name, "solve_threads")) { *value = de::get_solve_threads(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 

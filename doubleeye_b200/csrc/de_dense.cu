@@ -649,7 +649,7 @@ __global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b, int nstage
 // k_solve: the row solve, core/include/doubleeye/dense_solve.hpp:213-452 (K = 2,
 // candidates from the cost stage), plus the --out-conf planes and the confidence
 // (:158-171).  One CTA per row; shared-memory working set ~53 bytes per pixel.
-constexpr int kSolveThreads = 256;
+
 
 __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }
 __device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }
@@ -663,8 +663,9 @@ __device__ float confidence_dev(float s1, float s2, float lambda, float lrc, flo
   return (lrc > tol) ? fmin_ref(p, 0.35f) : p;
 }
 
+template <int kSolveThreads>
 __device__ __forceinline__ void block_excl_scan(int* a, int n, int* warp_sums) {
-  // exclusive scan of a[0..n) in place, a[n] = total; 256 threads, contiguous chunks
+  // exclusive scan of a[0..n) in place, a[n] = total; contiguous chunks per thread
   const int tid = threadIdx.x;
   const int per = (n + kSolveThreads - 1) / kSolveThreads;
   const int lo = min(n, tid * per), hi = min(n, lo + per);
@@ -696,7 +697,7 @@ __device__ __forceinline__ void block_excl_scan(int* a, int n, int* warp_sums) {
   __syncthreads();
 }
 
-template <bool REF_LAYOUT>
+template <bool REF_LAYOUT, int kSolveThreads>
 __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   extern __shared__ __align__(128) uint8_t smem[];
   const int item = blockIdx.x;
@@ -706,25 +707,28 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   const int y = item - b.solve_prefix[pi];
   const int dmin = cfg.dmin, hw = cfg.hw, hh = cfg.hh;
   const float lambda = cfg.lambda, gamma = cfg.gamma, damping = cfg.damping, keep = cfg.keep;
-  // shared layout (bytes per pixel): cs 8, beta 8, rho 8, margin 4, best 4, start 4,
-  // cur 4, items 4, lo 4, hi 4, cd 2, rev 2, cn 1, bestj 1, win 1  = 59
-  float* s_cs = reinterpret_cast<float*>(smem);          // [2W] item = 2x + j
-  float* s_beta = s_cs + 2 * W;                           // [2W]
-  float* s_rho = s_beta + 2 * W;                          // [2W]
-  float* s_margin = s_rho + 2 * W;                        // [W]
-  float* s_best = s_margin + W;                           // [W]
+  // Candidate state lives in bucket-sorted POSITION order: the members of a right
+  // pixel's bucket are contiguous, candidates that claim no right pixel follow them.
+  // Shared bytes per pixel: cs 8, beta 8, rho 8, lohi 8, item 4, pos 4, margin 4,
+  // best 4, start 4, cur 4, cd 2, rev 2, cn 1, bestj 1, win 1 = 63.
+  float* __restrict__ s_cs = reinterpret_cast<float*>(smem);          // [2W] by position
+  float* __restrict__ s_beta = s_cs + 2 * W;                           // [2W] by position
+  float* __restrict__ s_rho = s_beta + 2 * W;                          // [2W] by position (pixel-order cs first)
+  int* __restrict__ s_lohi = reinterpret_cast<int*>(s_rho + 2 * W);    // [2W] bucket bounds lo | hi << 16, -1 none
+  float* __restrict__ s_margin = reinterpret_cast<float*>(s_lohi + 2 * W);   // [W]
+  float* __restrict__ s_best = s_margin + W;                           // [W]
   int* s_start = reinterpret_cast<int*>(s_best + W);      // [W+1]
   int* s_cur = s_start + W + 1;                           // [W]
-  int16_t* s_items = reinterpret_cast<int16_t*>(s_cur + W);   // [2W] sorted by bucket
-  int16_t* s_lo = s_items + 2 * W;                        // [2W] bucket bounds of a position
-  int16_t* s_hi = s_lo + 2 * W;                           // [2W]
-  uint8_t* s_cd = reinterpret_cast<uint8_t*>(s_hi + 2 * W);  // [2W] k (valid for j < cn)
-  int16_t* s_rev = reinterpret_cast<int16_t*>(s_cd + 2 * W + (W & 1) * 2);  // [W]
+  int16_t* s_item = reinterpret_cast<int16_t*>(s_cur + W);   // [2W] position -> 2x + j
+  int16_t* s_pos = s_item + 2 * W;                        // [2W] 2x + j -> position
+  uint8_t* s_cd = reinterpret_cast<uint8_t*>(s_pos + 2 * W);  // [2W] k (valid for j < cn)
+  int16_t* s_rev = reinterpret_cast<int16_t*>(s_cd + 2 * W);  // [W]
   int8_t* s_cn = reinterpret_cast<int8_t*>(s_rev + W);    // [W]
   int8_t* s_bestj = s_cn + W;                             // [W]
   uint8_t* s_win = reinterpret_cast<uint8_t*>(s_bestj + W);  // [W]
+  float* s_cspx = s_rho;                                  // pixel-order cs until the sort
   __shared__ int warp_sums[kSolveThreads / 32];
-  __shared__ int s_nitems;
+  __shared__ int s_nitems, s_extra;
   const int tid = threadIdx.x;
   const bool row_ok = y >= hh && y < H - hh;
   const size_t row = size_t(y) * W;
@@ -744,7 +748,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       if (a) { c0 = float(int32_t(a >> 8) - 32768) * q; k0 = 255 - int(a & 255u); n = 1; }
       if (bb) { c1 = float(int32_t(bb >> 8) - 32768) * q; k1 = 255 - int(bb & 255u); n = 2; }
     }
-    reinterpret_cast<float2*>(s_cs)[x] = make_float2(c0, c1);
+    reinterpret_cast<float2*>(s_cspx)[x] = make_float2(c0, c1);
     s_cd[2 * x] = uint8_t(k0);
     s_cd[2 * x + 1] = uint8_t(k1);
     s_cn[x] = int8_t(n);
@@ -753,13 +757,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     s_margin[x] = m;
     if (P.margin) P.margin[row + x] = m;
     s_start[x] = 0;
-    reinterpret_cast<float2*>(s_beta)[x] = make_float2(0.f, 0.f);
-    reinterpret_cast<float2*>(s_rho)[x] = make_float2(0.f, 0.f);
     s_win[x] = 0;
   }
-  if (tid == 0) s_start[W] = 0;
+  if (tid == 0) { s_start[W] = 0; s_extra = 0; }
   __syncthreads();
-  // 2. claimant buckets by right pixel, counting sort (:270-284); order inside a
+  // 2. claimant buckets by right pixel, counting sort (:270-284); the order inside a
   //    bucket is free: only its maxima are ever read
   for (int x = tid; x < W; x += kSolveThreads)
     for (int j = 0; j < s_cn[x]; ++j) {
@@ -767,56 +769,70 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       if (xr >= 0) atomicAdd(&s_start[xr], 1);
     }
   __syncthreads();
-  block_excl_scan(s_start, W, warp_sums);
+  block_excl_scan<kSolveThreads>(s_start, W, warp_sums);
   for (int xr = tid; xr < W; xr += kSolveThreads) s_cur[xr] = s_start[xr];
   if (tid == 0) s_nitems = s_start[W];
   __syncthreads();
-  for (int x = tid; x < W; x += kSolveThreads)
-    for (int j = 0; j < s_cn[x]; ++j) {
-      const int xr = x - (dmin + s_cd[2 * x + j]);
-      if (xr >= 0) {
-        const int p = atomicAdd(&s_cur[xr], 1);
-        s_items[p] = int16_t(2 * x + j);
-        s_lo[p] = int16_t(s_start[xr]);
-        s_hi[p] = int16_t(s_start[xr + 1]);
-      }
-    }
-  __syncthreads();
   const int nitems = s_nitems;
+  for (int x = tid; x < W; x += kSolveThreads) {
+    const int n = s_cn[x];
+    for (int j = 0; j < n; ++j) {
+      const int xr = x - (dmin + s_cd[2 * x + j]);
+      int p, lohi = -1;
+      if (xr >= 0) {
+        p = atomicAdd(&s_cur[xr], 1);
+        lohi = s_start[xr] | (s_start[xr + 1] << 16);
+      } else {
+        p = nitems + atomicAdd(&s_extra, 1);
+      }
+      s_item[p] = int16_t(2 * x + j);
+      s_pos[2 * x + j] = int16_t(p);
+      s_cs[p] = s_cspx[2 * x + j];
+      s_lohi[p] = lohi;
+    }
+  }
+  __syncthreads();
+  const int nall = nitems + s_extra;
+  for (int p = tid; p < nall; p += kSolveThreads) { s_beta[p] = 0.f; s_rho[p] = 0.f; }
   // 3. reverse match over the surviving candidates (:303-313): first maximum in x order
   for (int xr = tid; xr < W; xr += kSolveThreads) {
     int bd = -1, bi = 1 << 30;
     float bv = kNegBig;
     for (int p = s_start[xr]; p < s_start[xr + 1]; ++p) {
-      const int idx = s_items[p];
-      const float v = s_cs[idx];
+      const int idx = s_item[p];
+      const float v = s_cs[p];
       if (v > bv || (v == bv && idx < bi)) { bv = v; bd = s_cd[idx]; bi = idx; }
     }
     s_rev[xr] = int16_t(bd);
   }
-  // 4. damped max-sum iterations (:318-341).  rho per pixel; beta per bucket member,
-  //    "max over the bucket excluding me" read directly from the other members.
+  // 4. damped max-sum iterations (:318-341): rho per pixel (its partner's beta through
+  //    the position table), beta per bucket position ("max over my bucket excluding me"
+  //    over a contiguous run of rho)
   for (int it = 0; it < cfg.iters; ++it) {
     __syncthreads();
     for (int x = tid; x < W; x += kSolveThreads) {
       const int n = s_cn[x];
       if (n == 0) continue;
-      const float2 cs2 = reinterpret_cast<const float2*>(s_cs)[x];
-      const float2 be = reinterpret_cast<const float2*>(s_beta)[x];
-      float2 rh = reinterpret_cast<const float2*>(s_rho)[x];
-      const float ex0 = (n == 2) ? be.y : kNegBig;
-      rh.x = keep * (cs2.x - fmax_ref(lambda, ex0)) + damping * rh.x;
-      if (n == 2) rh.y = keep * (cs2.y - fmax_ref(lambda, be.x)) + damping * rh.y;
-      reinterpret_cast<float2*>(s_rho)[x] = rh;
+      const int p0 = s_pos[2 * x];
+      if (n == 1) {
+        s_rho[p0] = keep * (s_cs[p0] - lambda) + damping * s_rho[p0];
+      } else {
+        const int p1 = s_pos[2 * x + 1];
+        const float b0 = s_beta[p0], b1 = s_beta[p1];
+        const float r0 = keep * (s_cs[p0] - fmax_ref(lambda, b1)) + damping * s_rho[p0];
+        const float r1 = keep * (s_cs[p1] - fmax_ref(lambda, b0)) + damping * s_rho[p1];
+        s_rho[p0] = r0;
+        s_rho[p1] = r1;
+      }
     }
     __syncthreads();
     for (int p = tid; p < nitems; p += kSolveThreads) {
-      const int idx = s_items[p];
-      const int lo = s_lo[p], hi = s_hi[p];
+      const int lohi = s_lohi[p];
+      const int lo = lohi & 0xFFFF, hi = lohi >> 16;
       float ex = kNegBig;
       for (int r = lo; r < hi; ++r)
-        if (r != p) ex = fmax_ref(ex, s_rho[s_items[r]]);
-      s_beta[idx] = keep * (s_cs[idx] - fmax_ref(gamma, ex)) + damping * s_beta[idx];
+        if (r != p) ex = fmax_ref(ex, s_rho[r]);
+      s_beta[p] = keep * (s_cs[p] - fmax_ref(gamma, ex)) + damping * s_beta[p];
     }
   }
   __syncthreads();
@@ -826,15 +842,16 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     int bj = -1;
     const int n = s_cn[x];
     for (int j = 0; j < n; ++j) {
-      const float c = s_cs[2 * x + j];
+      const int p = s_pos[2 * x + j];
+      const float c = s_cs[p];
       if (c <= lambda) continue;
-      const float bel = (cfg.iters > 0) ? (s_beta[2 * x + j] + s_rho[2 * x + j] - c) : c;
+      const float bel = (cfg.iters > 0) ? (s_beta[p] + s_rho[p] - c) : c;
       if (bel > best) { best = bel; bj = j; }
     }
     if (bj >= 0 && cfg.min_margin > 0.f && s_margin[x] < cfg.min_margin) bj = -1;
     if (bj >= 0 && cfg.min_ratio > 0.f) {
-      const float s2 = (n > 1) ? fmax_ref(s_cs[2 * x + 1], lambda) : lambda;
-      const float c1 = fmax_ref(1.f - s_cs[2 * x], 1e-6f);
+      const float s2 = (n > 1) ? fmax_ref(s_cs[s_pos[2 * x + 1]], lambda) : lambda;
+      const float c1 = fmax_ref(1.f - s_cs[s_pos[2 * x]], 1e-6f);
       if ((1.f - s2) / c1 < cfg.min_ratio) bj = -1;
     }
     s_best[x] = best;
@@ -848,7 +865,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     int wx = -1;
     float wb = 0.f;
     for (int p = s_start[xr]; p < s_start[xr + 1]; ++p) {
-      const int idx = s_items[p];
+      const int idx = s_item[p];
       const int x = idx >> 1, j = idx & 1;
       if (s_bestj[x] != j) continue;
       const float bv = s_best[x];
@@ -863,7 +880,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   for (int x = tid; x < W; x += kSolveThreads) {
     float dl = __int_as_float(0x7fc00000);
     const int n = s_cn[x];
-    const float2 cs2 = reinterpret_cast<const float2*>(s_cs)[x];
+    const float2 cs2 = make_float2(n > 0 ? s_cs[s_pos[2 * x]] : kNegBig,
+                                   n > 1 ? s_cs[s_pos[2 * x + 1]] : kNegBig);
     if (s_win[x]) {
       const int j = s_bestj[x];
       const int d = dmin + s_cd[2 * x + j];
@@ -965,7 +983,7 @@ size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   return (s + 15) & ~size_t(15);
 }
 
-size_t solve_smem(int W) { return size_t(W) * 59 + 64; }
+size_t solve_smem(int W) { return size_t(W) * 63 + 64; }
 
 template <typename K>
 cudaError_t set_smem(K kernel, size_t bytes) {
@@ -986,6 +1004,7 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
 struct de_cfg_hw { int hw, dmin; };
 int g_cols_stage_kb = 32;         // column kernel: shared bytes for the row ring
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
+int g_solve_threads = 256;        // threads per row in the solve
 
 template <bool PACKED, int TS, int G>
 cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
@@ -1040,6 +1059,8 @@ cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   return cudaSuccess;
 }
 
+void set_solve_threads(int v) { g_solve_threads = (v == 128 || v == 512) ? v : 256; }
+int get_solve_threads() { return g_solve_threads; }
 void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }
 int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
 
@@ -1099,13 +1120,18 @@ cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref, cudaS
   for (int i = 0; i < b.n; ++i) maxW = maxW > b.p[i].W ? maxW : b.p[i].W;
   const size_t sm = solve_smem(maxW);
   cudaError_t e;
-  if (from_ref) {
-    if ((e = set_smem(k_solve<true>, sm)) != cudaSuccess) return e;
-    k_solve<true><<<items, kSolveThreads, sm, s>>>(cfg, b);
-  } else {
-    if ((e = set_smem(k_solve<false>, sm)) != cudaSuccess) return e;
-    k_solve<false><<<items, kSolveThreads, sm, s>>>(cfg, b);
+  auto go = [&](auto kern, int nt) -> cudaError_t {
+    cudaError_t e2 = set_smem(kern, sm);
+    if (e2 != cudaSuccess) return e2;
+    kern<<<items, nt, sm, s>>>(cfg, b);
+    return cudaSuccess;
+  };
+  switch (g_solve_threads) {
+    case 128: e = from_ref ? go(k_solve<true, 128>, 128) : go(k_solve<false, 128>, 128); break;
+    case 512: e = from_ref ? go(k_solve<true, 512>, 512) : go(k_solve<false, 512>, 512); break;
+    default: e = from_ref ? go(k_solve<true, 256>, 256) : go(k_solve<false, 256>, 256); break;
   }
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

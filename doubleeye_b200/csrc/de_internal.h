@@ -92,6 +92,8 @@ cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref_layout
 void set_rows_ctas_per_sm(int v);
 int get_rows_ctas_per_sm();
 void set_cols_kt(int v);
+void set_solve_threads(int v);
+int get_solve_threads();
 void set_cols_stage_kb(int v);
 int get_cols_stage_kb();
 int get_cols_kt();

@@ -162,7 +162,9 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *   "cols_kt"           disparities per lane in the column kernel: 8, 16, or 0 to
  *                       choose by batch size (default 0)
  *   "cols_stage_kb"     shared memory (KB) for the column kernel's row ring; its
- *                       depth is this over one row of a tile (default 32) */
+ *                       depth is this over one row of a tile (default 32)
+ *   "solve_threads"     threads per image row in the row solve: 128, 256 or 512
+ *                       (default 256) */
 DE_API int de_set_param(const char* name, int value);
 DE_API int de_get_param(const char* name, int* value);
 

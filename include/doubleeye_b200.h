@@ -27,7 +27,6 @@
  *   core/include/doubleeye/preproc.hpp:96-97         census_at      -> de_census_at_dev
  *   core/include/doubleeye/preproc.hpp:202-204       detect_keypoints_fast -> de_detect_fast_dev
  *   core/include/doubleeye/match.hpp:221-226         match_masda    -> de_match_masda_dev
- *   article/masda_stereo.py:453-492                  masda_sparse   -> de_masda_edges_dev
  */
 #ifndef DOUBLEEYE_B200_H
 #define DOUBLEEYE_B200_H
@@ -207,6 +206,37 @@ typedef struct de_match_stats {
   float final_max_delta;
   int oscillating;
 } de_match_stats;
+
+/* census_at (core/src/preproc.cpp:142-162) at n keypoints, each at
+ * (int(x + 0.5), int(y + 0.5)) as core/tools/de_match.cpp:228-232 rounds them.
+ * desc[k] = 0 and ok[k] = 0 where the window leaves the image; ok may be NULL.
+ * n_dev, if not NULL, is a device count that limits n (a detector's output). */
+DE_API int de_census_at_dev(const uint8_t* img, int W, int H, const de_keypoint* kp, int n,
+                            const int* n_dev, int hw, int hh, uint64_t* desc, uint8_t* ok,
+                            void* stream);
+
+/* detect_keypoints_fast (core/src/preproc.cpp:442-545).  Writes at most cap keypoints
+ * to out in the reference's order (grid cells row-major, each cell's strongest
+ * per_cell first) and the full count to the device int *n_out (-1 if the
+ * suppression did not settle, which needs a pathological chain of > 65536 points).
+ * Images 16..4096 x 16..8192, cell <= 128. */
+DE_API int de_detect_workspace_bytes(int W, int H, const de_det_cfg* cfg, size_t* bytes);
+DE_API int de_detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* cfg,
+                              de_keypoint* out, int cap, int* n_out, void* workspace,
+                              size_t bytes, void* stream);
+
+/* match_masda (core/include/doubleeye/match.hpp:221-226, core/src/match.cpp:334-417)
+ * on device keypoints and descriptors.  nl/nr are the array sizes; nl_dev/nr_dev,
+ * if not NULL, are device counts that limit them (so a detector's output feeds
+ * this call without a host round trip).  Matches go to out (at most cap) in the
+ * reference's emission order; the count to the device int *n_out; stats (device,
+ * may be NULL) as MatchStats.  One CTA solves the problem; nr <= 16384. */
+DE_API int de_match_workspace_bytes(int nl, int nr, const de_match_cfg* cfg, size_t* bytes);
+DE_API int de_match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
+                              const int* nl_dev, const de_keypoint* kr, const uint64_t* dr,
+                              int nr, const int* nr_dev, const de_match_cfg* cfg, de_match* out,
+                              int cap, int* n_out, de_match_stats* stats, void* workspace,
+                              size_t bytes, void* stream);
 
 /* ---- dense, host pointers, context-owned memory, synchronous ----------------- */
 

@@ -50,6 +50,26 @@ void or_dense(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int 
 float or_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol);
 unsigned or_confidence_u8(float s1, float s2, float lambda, float lrc, float lrc_tol);
 
+/* sparse path (de_oracle_sparse.c) */
+uint64_t or_census_at(const uint8_t* img, int W, int H, int x, int y, int hw, int hh,
+                      int* ok);
+int or_is_fast_corner(const uint8_t* img, int W, int H, int x, int y, int thr);
+float or_shi_tomasi_at(const uint8_t* img, int W, int H, int x, int y, int gw);
+float or_local_std_at(const uint8_t* img, int W, int H, int x, int y, int window);
+int or_detect_fast(const uint8_t* img, int W, int H, const de_det_cfg* c, de_keypoint* out,
+                   int cap);
+float or_pair_score(const de_keypoint* l, const de_keypoint* r, uint64_t dl, uint64_t dr,
+                    const de_match_cfg* c);
+int or_match_masda(const de_keypoint* kl, const uint64_t* dl, int nl, const de_keypoint* kr,
+                   const uint64_t* dr, int nr, const de_match_cfg* c, de_match* out, int cap,
+                   de_match_stats* st);
+int or_match_edges(const de_keypoint* kl, const uint64_t* dl, int nl, const de_keypoint* kr,
+                   const uint64_t* dr, int nr, const de_match_cfg* c, int* ei, int* ej,
+                   float* s, int cap);
+int or_masda_edges(const int64_t* ei, const int64_t* ej, const double* se, int64_t E,
+                   int64_t m, int64_t n, double lam, double gam, int iters, double damping,
+                   double eps, int64_t* assign, double* hist);
+
 #ifdef __cplusplus
 }
 #endif

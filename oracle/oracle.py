@@ -65,6 +65,11 @@ class DeMatchStats(C.Structure):
                 ("final_max_delta", C.c_float), ("oscillating", C.c_int)]
 
 
+MATCH_DTYPE = np.dtype([("left", np.int32), ("right", np.int32), ("score", np.float32),
+                        ("belief", np.float32), ("disparity", np.float32),
+                        ("dy", np.float32), ("margin", np.float32)])
+
+
 def default_cfg(**kw) -> DeCfg:
     """Reference defaults, core/include/doubleeye/dense_solve.hpp:34-70."""
     c = DeCfg(dmin=1, dmax=60, iters=0, sigma_s=8.0, sigma_r=0.2, ad=0.15, ad_trunc=10,
@@ -148,6 +153,12 @@ class Oracle:
         L.or_census_at.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                    C.c_int, C.POINTER(C.c_int)]
         L.or_census_at.restype = C.c_uint64
+        L.or_is_fast_corner.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_int]
+        L.or_shi_tomasi_at.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.or_shi_tomasi_at.restype = C.c_float
+        L.or_local_std_at.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.or_local_std_at.restype = C.c_float
         L.or_detect_fast.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(DeDetCfg),
                                      C.c_void_p, C.c_int]
         L.or_detect_fast.restype = C.c_int
@@ -155,6 +166,76 @@ class Oracle:
                                      C.c_int, C.POINTER(DeMatchCfg), C.c_void_p, C.c_int,
                                      C.POINTER(DeMatchStats)]
         L.or_match_masda.restype = C.c_int
+        L.or_match_edges.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                     C.c_int, C.POINTER(DeMatchCfg), C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_int]
+        L.or_match_edges.restype = C.c_int
+        L.or_masda_edges.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64,
+                                     C.c_int64, C.c_double, C.c_double, C.c_int, C.c_double,
+                                     C.c_double, C.c_void_p, C.c_void_p]
+        L.or_masda_edges.restype = C.c_int
+
+    # -- sparse --------------------------------------------------------------------
+    def census_at(self, img, x, y, hw=3, hh=3):
+        img = np.ascontiguousarray(img, np.uint8)
+        H, W = img.shape
+        ok = C.c_int()
+        v = self.lib.or_census_at(img.ctypes.data, W, H, int(x), int(y), hw, hh, C.byref(ok))
+        return int(v), bool(ok.value)
+
+    def detect_fast(self, img, det: DeDetCfg | None = None) -> np.ndarray:
+        """Keypoints as an (n, 4) float32 array of x, y, response, local_std."""
+        img = np.ascontiguousarray(img, np.uint8)
+        H, W = img.shape
+        det = det or default_det_cfg()
+        cap = 1 << 16
+        out = np.zeros((cap, 4), np.float32)
+        n = self.lib.or_detect_fast(img.ctypes.data, W, H, C.byref(det), out.ctypes.data, cap)
+        return out[:min(n, cap)].copy()
+
+    def match_masda(self, kl, dl, kr, dr, cfg: DeMatchCfg | None = None):
+        """Matches as a structured array (left, right, score, belief, disparity, dy,
+        margin) and the stats."""
+        cfg = cfg or default_match_cfg()
+        kl = np.ascontiguousarray(kl, np.float32).reshape(-1, 4)
+        kr = np.ascontiguousarray(kr, np.float32).reshape(-1, 4)
+        dl = np.ascontiguousarray(dl, np.uint64)
+        dr = np.ascontiguousarray(dr, np.uint64)
+        cap = max(1, len(kl))
+        out = np.zeros(cap, MATCH_DTYPE)
+        st = DeMatchStats()
+        n = self.lib.or_match_masda(kl.ctypes.data, dl.ctypes.data, len(kl), kr.ctypes.data,
+                                    dr.ctypes.data, len(kr), C.byref(cfg), out.ctypes.data,
+                                    cap, C.byref(st))
+        return out[:n].copy(), st
+
+    def match_edges(self, kl, dl, kr, dr, cfg: DeMatchCfg | None = None):
+        cfg = cfg or default_match_cfg()
+        kl = np.ascontiguousarray(kl, np.float32).reshape(-1, 4)
+        kr = np.ascontiguousarray(kr, np.float32).reshape(-1, 4)
+        dl = np.ascontiguousarray(dl, np.uint64)
+        dr = np.ascontiguousarray(dr, np.uint64)
+        cap = max(1, len(kl) * max(1, cfg.max_candidates))
+        ei = np.zeros(cap, np.int32)
+        ej = np.zeros(cap, np.int32)
+        s = np.zeros(cap, np.float32)
+        n = self.lib.or_match_edges(kl.ctypes.data, dl.ctypes.data, len(kl), kr.ctypes.data,
+                                    dr.ctypes.data, len(kr), C.byref(cfg), ei.ctypes.data,
+                                    ej.ctypes.data, s.ctypes.data, cap)
+        return ei[:n].copy(), ej[:n].copy(), s[:n].copy()
+
+    def masda_edges(self, ei, ej, se, m, n, lam=-0.1, gam=-0.1, iters=30, damping=0.4,
+                    eps=1e-5):
+        """masda_sparse in float64 with a stable belief order: (assign[m], hist)."""
+        ei = np.ascontiguousarray(ei, np.int64)
+        ej = np.ascontiguousarray(ej, np.int64)
+        se = np.ascontiguousarray(se, np.float64)
+        assign = np.zeros(max(1, m), np.int64)
+        hist = np.zeros(max(1, iters), np.float64)
+        k = self.lib.or_masda_edges(ei.ctypes.data, ej.ctypes.data, se.ctypes.data, len(se),
+                                    m, n, lam, gam, iters, damping, eps, assign.ctypes.data,
+                                    hist.ctypes.data)
+        return assign[:m].copy(), hist[:k].copy()
 
     # -- dense ---------------------------------------------------------------------
     def census(self, img: np.ndarray, hw: int = 3, hh: int = 3) -> np.ndarray:
@@ -350,6 +431,49 @@ class Reference:
 
     def confidence(self, s1, s2, lam, lrc=0.0, tol=1.0):
         return self.lib.ref_confidence(s1, s2, lam, lrc, tol)
+
+    def census_at(self, img, x, y, hw=3, hh=3):
+        img = np.ascontiguousarray(img, np.uint8)
+        H, W = img.shape
+        ok = C.c_int()
+        v = self.lib.ref_census_at(img.ctypes.data, W, H, int(x), int(y), hw, hh, C.byref(ok))
+        return int(v), bool(ok.value)
+
+    def detect_fast(self, img, det: DeDetCfg | None = None) -> np.ndarray:
+        img = np.ascontiguousarray(img, np.uint8)
+        H, W = img.shape
+        det = det or default_det_cfg()
+        cap = 1 << 16
+        out = np.zeros((cap, 4), np.float32)
+        n = self.lib.ref_detect_fast(img.ctypes.data, W, H, C.byref(det), out.ctypes.data, cap)
+        return out[:min(n, cap)].copy()
+
+    def match_masda(self, kl, dl, kr, dr, cfg: DeMatchCfg | None = None):
+        cfg = cfg or default_match_cfg()
+        kl = np.ascontiguousarray(kl, np.float32).reshape(-1, 4)
+        kr = np.ascontiguousarray(kr, np.float32).reshape(-1, 4)
+        dl = np.ascontiguousarray(dl, np.uint64)
+        dr = np.ascontiguousarray(dr, np.uint64)
+        cap = max(1, len(kl))
+        out = np.zeros(cap, MATCH_DTYPE)
+        st = DeMatchStats()
+        n = self.lib.ref_match_masda(kl.ctypes.data, dl.ctypes.data, len(kl), kr.ctypes.data,
+                                     dr.ctypes.data, len(kr), C.byref(cfg), out.ctypes.data,
+                                     cap, C.byref(st))
+        return out[:n].copy(), st
+
+    def match_brute_force(self, kl, dl, kr, dr, cfg: DeMatchCfg | None = None):
+        cfg = cfg or default_match_cfg()
+        kl = np.ascontiguousarray(kl, np.float32).reshape(-1, 4)
+        kr = np.ascontiguousarray(kr, np.float32).reshape(-1, 4)
+        dl = np.ascontiguousarray(dl, np.uint64)
+        dr = np.ascontiguousarray(dr, np.uint64)
+        cap = max(1, len(kl))
+        out = np.zeros(cap, MATCH_DTYPE)
+        n = self.lib.ref_match_brute_force(kl.ctypes.data, dl.ctypes.data, len(kl),
+                                           kr.ctypes.data, dr.ctypes.data, len(kr),
+                                           C.byref(cfg), out.ctypes.data, cap)
+        return out[:n].copy()
 
     def confidence_u8(self, s1, s2, lam, lrc=0.0, tol=1.0):
         return self.lib.ref_confidence_u8(s1, s2, lam, lrc, tol)

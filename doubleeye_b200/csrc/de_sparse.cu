@@ -9,9 +9,9 @@
 //
 // The reference is sequential C++.  Here:
 //   * the detector is one pass over pixels (corner test + response), then the
-//     greedy strongest-first suppression as rounds of local decisions (a candidate
-//     is kept once every stronger candidate in its square is decided and none of
-//     them is kept), which yields exactly the sequential result; then one CTA per
+//     greedy strongest-first suppression resolved per candidate (a point is kept
+//     iff none of its stronger neighbours is kept, settled depth first by any thread
+//     that needs it), which yields exactly the sequential result; then one CTA per
 //     grid cell refines its survivors and keeps the strongest per_cell.
 //   * one CTA solves one matching problem end to end: y-sort of the right points
 //     (bitonic, shared memory), candidate rows (one thread per left point), CSR/CSC
@@ -37,7 +37,6 @@ namespace {
 constexpr float kNegBig = -1e30f;
 constexpr int kSortMax = 16384;          // right keypoints per problem (shared-memory sort)
 constexpr int kMaxCell = 128;            // detector grid cell edge
-constexpr int kNmsMaxRounds = 1 << 16;   // suppression rounds (each decides >= 1 point)
 
 __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }
 
@@ -216,49 +215,66 @@ __global__ void k_fast(const uint8_t* __restrict__ img, int W, int H, int border
   if (is_cand) d.listA[base + __popc(ballot & ((1u << lane) - 1u))] = y * W + x;
 }
 
-// Stage 2: greedy suppression, strongest first, as rounds.  One CTA per image.
-__global__ void __launch_bounds__(1024) k_nms(int W, int H, int rad, DetWs d) {
-  __shared__ int s_next;
-  int* cur = d.listA;
-  int* nxt = d.listB;
-  int n = d.counters[0];
-  const volatile uint8_t* st = d.state;
-  int round = 0;
-  for (; n > 0 && round < kNmsMaxRounds; ++round) {
-    if (threadIdx.x == 0) s_next = 0;
-    __syncthreads();
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      const int i = cur[k];
-      const int x = i % W, y = i / W;
-      const float r = d.resp[i];
-      bool supp = false, pend = false;
-      for (int dy = -rad; dy <= rad && !supp; ++dy) {
-        const int py = y + dy;
-        if (py < 0 || py >= H) continue;
-        for (int dx = -rad; dx <= rad; ++dx) {
-          const int px = x + dx;
-          if (px < 0 || px >= W) continue;
-          const int j = py * W + px;
-          const int s = st[j];
-          if (j == i || s == 0 || s == 3) continue;
-          const float rj = d.resp[j];
-          if (!(rj > r || (rj == r && j < i))) continue;   // not stronger
-          if (s == 2) { supp = true; break; }
-          pend = true;
+// Stage 2: greedy suppression, strongest first.  The sequential rule (keep a point
+// unless an already kept, stronger point lies in its square) makes a point's fate a
+// function of the fates of its stronger neighbours only: kept iff none of them is
+// kept.  Each thread settles one candidate by resolving undecided stronger
+// neighbours depth first and records every settled fate in the state map.  Threads
+// never wait for one another: one that reads a stale "undecided" recomputes that
+// fate itself and necessarily reaches the same value, so concurrent writes agree.
+constexpr int kNmsStack = 32;
+constexpr int kNmsGuard = 1 << 22;       // visits per thread before it gives up
+
+__device__ __forceinline__ bool stronger(float rj, int j, float r, int i) {
+  return rj > r || (rj == r && j < i);    // response desc, then scan order
+}
+
+__global__ void __launch_bounds__(256) k_nms(int W, int H, int rad, DetWs d) {
+  const int n = d.counters[0];
+  volatile uint8_t* st = d.state;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int root = d.listA[q];
+    int stack[kNmsStack];
+    int guard = 0;
+    while (st[root] == 1) {
+      int sp = 0;
+      stack[sp++] = root;
+      while (sp > 0) {
+        if (++guard > kNmsGuard) {
+          d.counters[1] = 1;
+          return;
         }
+        const int t = stack[sp - 1];
+        if (st[t] != 1) { --sp; continue; }
+        const int x = t % W, y = t / W;
+        const float r = d.resp[t];
+        bool supp = false;
+        int pend = -1;
+        for (int dy = -rad; dy <= rad && !supp; ++dy) {
+          const int py = y + dy;
+          if (py < 0 || py >= H) continue;
+          for (int dx = -rad; dx <= rad; ++dx) {
+            const int px = x + dx;
+            if (px < 0 || px >= W) continue;
+            const int j = py * W + px;
+            const int s = st[j];
+            if (s == 0 || s == 3 || j == t) continue;
+            if (!stronger(d.resp[j], j, r, t)) continue;
+            if (s == 2) { supp = true; break; }
+            pend = j;
+          }
+        }
+        if (supp) { st[t] = 3; --sp; continue; }
+        if (pend < 0) { st[t] = 2; --sp; continue; }
+        if (sp == kNmsStack) {              // keep the deeper half; the rest is redone
+#pragma unroll
+          for (int k = 0; k < kNmsStack / 2; ++k) stack[k] = stack[k + kNmsStack / 2];
+          sp = kNmsStack / 2;
+        }
+        stack[sp++] = pend;
       }
-      if (supp) d.state[i] = 3;
-      else if (!pend) d.state[i] = 2;
-      else nxt[atomicAdd(&s_next, 1)] = i;
     }
-    __syncthreads();
-    n = s_next;
-    int* t = cur;
-    cur = nxt;
-    nxt = t;
-    __syncthreads();
   }
-  if (threadIdx.x == 0 && n > 0) d.counters[1] = 1;       // did not converge
 }
 
 // Stage 3: one CTA per grid cell.  Texture floor, sub-pixel, strongest per_cell.
@@ -867,7 +883,10 @@ int detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* c, de_ke
   const dim3 blk(32, 8), grd((W + 31) / 32, (H + 7) / 8);
   k_fast<<<grd, blk, 0, s>>>(img, W, H, border, c->fast_threshold, c->grad_window,
                              c->min_response, d);
-  k_nms<<<1, 1024, 0, s>>>(W, H, std::max(1, c->nms_radius), d);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  k_nms<<<sms * 8, 256, 0, s>>>(W, H, std::max(1, c->nms_radius), d);
   const int capk = ((cell + 1) / 2) * ((cell + 1) / 2);
   const size_t sm = size_t(capk) * (sizeof(de_keypoint) + sizeof(int));
   e = cudaFuncSetAttribute(k_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));

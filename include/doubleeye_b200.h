@@ -217,8 +217,9 @@ DE_API int de_census_at_dev(const uint8_t* img, int W, int H, const de_keypoint*
 
 /* detect_keypoints_fast (core/src/preproc.cpp:442-545).  Writes at most cap keypoints
  * to out in the reference's order (grid cells row-major, each cell's strongest
- * per_cell first) and the full count to the device int *n_out (-1 if the
- * suppression did not settle, which needs a pathological chain of > 65536 points).
+ * per_cell first) and the full count to the device int *n_out (-1 if resolving the
+ * strongest-first suppression exceeded its work bound, which takes a monotone
+ * response ramp thousands of points long).
  * Images 16..4096 x 16..8192, cell <= 128. */
 DE_API int de_detect_workspace_bytes(int W, int H, const de_det_cfg* cfg, size_t* bytes);
 DE_API int de_detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* cfg,

@@ -115,6 +115,26 @@ SIGNATURES = {
     "de_match_masda_dev": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, C.c_int, vp,
                                      C.POINTER(DeMatchCfg), vp, C.c_int, vp, vp, vp,
                                      C.c_size_t, vp]),
+    "de_masda_edges_workspace_bytes": (C.c_int, [C.c_longlong, C.c_longlong, C.c_longlong,
+                                                 C.POINTER(C.c_size_t)]),
+    "de_masda_edges_dev": (C.c_int, [vp, vp, vp, C.c_longlong, C.c_longlong, C.c_longlong,
+                                     C.c_double, C.c_double, C.c_int, C.c_double, C.c_double,
+                                     vp, vp, vp, vp, vp, C.c_size_t, vp]),
+    "de_masda_decide_dev": (C.c_int, [vp, vp, vp, vp, C.c_longlong, C.c_longlong,
+                                      C.c_longlong, C.c_double, vp, vp, C.c_size_t, vp]),
+    "de_seg_max_excluding_dev": (C.c_int, [vp, vp, C.c_longlong, C.c_longlong, vp, vp,
+                                           C.c_size_t, vp]),
+    "de_hamming_dev": (C.c_int, [vp, vp, C.c_longlong, vp, vp]),
+    "de_census_pts_dev": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_longlong, C.c_int, C.c_int,
+                                    vp, vp, vp]),
+    "de_build_problem_dev": (C.c_int, [vp, vp, C.c_longlong, vp, vp, C.c_longlong, C.c_float,
+                                       C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                       vp, vp]),
+    "de_edges_from_matrix_dev": (C.c_int, [vp, C.c_longlong, C.c_longlong, vp, vp, vp,
+                                           C.c_longlong, vp, vp, C.c_size_t, vp]),
+    "de_dense_problem_edges": (C.c_longlong, [C.c_int] * 6),
+    "de_dense_problem_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, vp, vp, vp, C.c_longlong, vp, C.c_size_t, vp]),
 }
 
 _lib = None

@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdoubleeye_b200.so")
 
-SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_serve.cu"]
+SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu", "de_serve.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -40,8 +40,15 @@ def sources():
     return [os.path.join(CSRC, s) for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
 
 
+def _stamp() -> str:
+    return " ".join(NVCC_FLAGS + [os.path.basename(s) for s in sources()])
+
+
 def stale() -> bool:
     if not os.path.exists(LIB):
+        return True
+    stamp = LIB + ".cmd"
+    if not os.path.exists(stamp) or open(stamp).read() != _stamp():
         return True
     t = os.path.getmtime(LIB)
     deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
@@ -58,6 +65,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)
+    with open(LIB + ".cmd", "w") as f:
+        f.write(_stamp())
     os.replace(tmp, LIB)
     return LIB
 

@@ -27,6 +27,9 @@
  *   core/include/doubleeye/preproc.hpp:96-97         census_at      -> de_census_at_dev
  *   core/include/doubleeye/preproc.hpp:202-204       detect_keypoints_fast -> de_detect_fast_dev
  *   core/include/doubleeye/match.hpp:221-226         match_masda    -> de_match_masda_dev
+ *   article/masda_stereo.py:392-492                  masda_sparse/decide -> de_masda_edges_dev,
+ *                                                    de_masda_decide_dev
+ *   article/dense_masda.py:39-79                     dense_problem  -> de_dense_problem_dev
  */
 #ifndef DOUBLEEYE_B200_H
 #define DOUBLEEYE_B200_H
@@ -238,6 +241,61 @@ DE_API int de_match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
                               int nr, const int* nr_dev, const de_match_cfg* cfg, de_match* out,
                               int cap, int* n_out, de_match_stats* stats, void* workspace,
                               size_t bytes, void* stream);
+
+/* ---- the Python entry points: edge-list MASDA in double precision ------------ */
+
+/* masda_sparse (article/masda_stereo.py:453-492) on device edge lists: ei/ej int64
+ * left/right node of each of E edges, se float64 scores; m left and n right nodes.
+ * float64 throughout, as NumPy.  assign[m] (device) = matched right node or -1;
+ * hist (device, >= iters doubles) gets the per-iteration largest message change and
+ * *n_hist (device) their count; belief (device, E doubles, may be NULL) the final
+ * beliefs.  Exact belief ties go to the lower edge index.  Blocks the calling
+ * thread while the greedy decision runs (it checks the remaining edge count between
+ * rounds).  E < 2^31. */
+DE_API int de_masda_edges_workspace_bytes(long long E, long long m, long long n,
+                                          size_t* bytes);
+DE_API int de_masda_edges_dev(const int64_t* ei, const int64_t* ej, const double* se,
+                              long long E, long long m, long long n, double lam, double gam,
+                              int iters, double damping, double eps, int64_t* assign,
+                              double* hist, int* n_hist, double* belief, void* workspace,
+                              size_t bytes, void* stream);
+/* decide (article/masda_stereo.py:392-414): greedy one-to-one in belief order over
+ * edges with finite belief and score > lam.  Same workspace as de_masda_edges_dev. */
+DE_API int de_masda_decide_dev(const int64_t* ei, const int64_t* ej, const double* se,
+                               const double* belief, long long E, long long m, long long n,
+                               double lam, int64_t* assign, void* workspace, size_t bytes,
+                               void* stream);
+/* _seg_max_excluding (article/masda_stereo.py:417-442); workspace >= 20*n + 1024 bytes. */
+DE_API int de_seg_max_excluding_dev(const double* vals, const int64_t* idx, long long E,
+                                    long long n, double* out, void* workspace, size_t bytes,
+                                    void* stream);
+/* hamming (article/masda_stereo.py:290-295): popcount(a ^ b) per element. */
+DE_API int de_hamming_dev(const uint64_t* a, const uint64_t* b, long long n, int32_t* out,
+                          void* stream);
+/* census (article/masda_stereo.py:264-284) at integer points xy[2k], xy[2k+1];
+ * 0 (and ok = 0) where the window leaves the image. */
+DE_API int de_census_pts_dev(const uint8_t* img, int W, int H, const int32_t* xy, long long n,
+                             int hw, int hh, uint64_t* out, uint8_t* ok, void* stream);
+/* build_problem (article/masda_stereo.py:305-326): the m x n float32 score matrix,
+ * -inf outside the epipolar band / disparity range; pl, pr are (x, y) float32 pairs;
+ * bits is the descriptor length the score is scaled by (48 in the reference). */
+DE_API int de_build_problem_dev(const float* pl, const uint64_t* dl, long long m,
+                                const float* pr, const uint64_t* dr, long long n, float max_dy,
+                                float dmin, float dmax, float sigma_y, float w_y, int bits,
+                                float* S, void* stream);
+/* to_edges (article/masda_stereo.py:445-450): finite entries of S in row-major order;
+ * *n_out (device int64) = their count, at most cap written; workspace >= 8*m + 256. */
+DE_API int de_edges_from_matrix_dev(const float* S, long long m, long long n, int64_t* ei,
+                                    int64_t* ej, double* se, long long cap, int64_t* n_out,
+                                    void* workspace, size_t bytes, void* stream);
+/* dense_problem (article/dense_masda.py:39-79): every interior pixel against every
+ * disparity dmin..dmax (0 <= dmin, at most 512 values) on its row, in the reference's
+ * order (disparity, then row, then column); se = (24 - Hamming)/24 as float32.
+ * de_dense_problem_edges gives the edge count; workspace >= 16*W*H + 512 bytes. */
+DE_API long long de_dense_problem_edges(int W, int H, int dmin, int dmax, int hw, int hh);
+DE_API int de_dense_problem_dev(const uint8_t* L, const uint8_t* R, int W, int H, int dmin,
+                                int dmax, int hw, int hh, int64_t* ei, int64_t* ej, float* se,
+                                long long cap, void* workspace, size_t bytes, void* stream);
 
 /* ---- dense, host pointers, context-owned memory, synchronous ----------------- */
 

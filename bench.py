@@ -162,8 +162,9 @@ def max_over_ranks(x: float, ws: int) -> float:
     return float(t.item())
 
 
-def cpu_baseline_sample(budget_s: float = 12.0, max_pairs: int = 24) -> dict:
-    """The reference's CPU path on this host's cores, bounded sample."""
+def cpu_baseline_sample(budget_s: float = 15.0, max_pairs: int = 400) -> dict:
+    """The reference's CPU path on this host's cores: as many pairs as fit in about
+    budget_s seconds (at least 3)."""
     from oracle import oracle as O
     nthreads = os.cpu_count() or 1
     pairs = make_pairs(3, 900)
@@ -178,7 +179,7 @@ def cpu_baseline_sample(budget_s: float = 12.0, max_pairs: int = 24) -> dict:
         kind, cores = "port", 1
     run(pairs[0])                                  # warm caches
     n, t0 = 0, time.perf_counter()
-    while n < max_pairs and time.perf_counter() - t0 < budget_s:
+    while n < max_pairs and (n < 3 or time.perf_counter() - t0 < budget_s):
         run(pairs[n % len(pairs)])
         n += 1
     dt = time.perf_counter() - t0

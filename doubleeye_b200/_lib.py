@@ -135,6 +135,17 @@ SIGNATURES = {
     "de_dense_problem_edges": (C.c_longlong, [C.c_int] * 6),
     "de_dense_problem_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, vp, vp, vp, C.c_longlong, vp, C.c_size_t, vp]),
+    "de_server_cfg_default": (None, [vp]),
+    "de_server_create": (C.c_int, [C.POINTER(DeCfg), vp, C.POINTER(vp)]),
+    "de_server_submit": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
+                                   C.POINTER(C.c_ulonglong)]),
+    "de_server_wait": (C.c_int, [vp, C.c_ulonglong, C.c_int, vp, vp, vp, vp, vp,
+                                 C.POINTER(C.c_double)]),
+    "de_server_stats": (C.c_int, [vp, vp]),
+    "de_server_reset_stats": (C.c_int, [vp]),
+    "de_server_last_disparity": (C.c_int, [vp, C.c_int, vp, C.c_int, C.c_int]),
+    "de_server_destroy": (C.c_int, [vp]),
+    "de_dedd_encode_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp, vp]),
 }
 
 _lib = None

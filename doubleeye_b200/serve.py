@@ -1,0 +1,195 @@
+"""Serving many camera streams: the Python side of the C-ABI server (de_server_*).
+
+``Server`` admits stereo pairs from any thread (host arrays, any supported size, a
+camera-stream id each), batches what is waiting onto the GPU as lanes free up, and
+returns each pair's disparity, margin, confidence and DEDD planes (Q4 disparity and
+confidence, as core/tools/de_dense_cuda.cu:729-746 encodes them).  Results are the
+plain pipeline's bit for bit.
+
+``simulate`` drives a server with camera streams at a frame rate with timing jitter
+(the serving workload: 16 streams at 30 Hz, 640x480 / 848x480 plus one 1280x720) and
+reports p50/p99 submit-to-result latency and throughput.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import threading
+import time
+from typing import Optional, Sequence
+
+import numpy as np
+
+from ._lib import DeCfg, check, lib
+
+
+class DeServerCfg(C.Structure):
+    _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_batch", C.c_int),
+                ("lanes", C.c_int)]
+
+
+class DeServerReport(C.Structure):
+    _fields_ = [("completed", C.c_ulonglong), ("failed", C.c_ulonglong),
+                ("batches", C.c_ulonglong), ("mean_batch", C.c_double),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("max_ms", C.c_double),
+                ("max_pending", C.c_size_t)]
+
+
+def _u8(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.uint8)
+    if a.ndim != 2:
+        raise ValueError("images must be 2-D uint8")
+    return a
+
+
+class Server:
+    def __init__(self, cfg: Optional[DeCfg] = None, device: int = 0,
+                 hbm_budget: int = 8 << 30, max_batch: int = 16, lanes: int = 2):
+        from .dense import Cfg
+        self.cfg = cfg or Cfg()
+        sc = DeServerCfg()
+        lib().de_server_cfg_default(C.byref(sc))
+        sc.device, sc.hbm_budget, sc.max_batch, sc.lanes = device, hbm_budget, max_batch, lanes
+        self._h = C.c_void_p()
+        check(lib().de_server_create(C.byref(self.cfg), C.byref(sc), C.byref(self._h)))
+        self._shape = {}
+        self._mu = threading.Lock()
+
+    def submit(self, stream: int, L, R, dmax: int = 0) -> int:
+        L, R = _u8(L), _u8(R)
+        H, W = L.shape
+        t = C.c_ulonglong()
+        check(lib().de_server_submit(self._h, int(stream), L.ctypes.data, R.ctypes.data, W, H,
+                                     int(dmax), C.byref(t)))
+        with self._mu:
+            self._shape[t.value] = (H, W)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> dict:
+        with self._mu:
+            H, W = self._shape[ticket]
+        out = dict(disp=np.empty((H, W), np.float32), margin=np.empty((H, W), np.float32),
+                   conf=np.empty((H, W), np.uint8), q4=np.empty((H, W), np.int16),
+                   qconf=np.empty((H, W), np.uint8))
+        lat = C.c_double()
+        check(lib().de_server_wait(self._h, C.c_ulonglong(ticket), int(timeout_ms),
+                                   out["disp"].ctypes.data, out["margin"].ctypes.data,
+                                   out["conf"].ctypes.data, out["q4"].ctypes.data,
+                                   out["qconf"].ctypes.data, C.byref(lat)))
+        with self._mu:
+            del self._shape[ticket]
+        out["latency_ms"] = lat.value
+        return out
+
+    def stats(self) -> dict:
+        r = DeServerReport()
+        check(lib().de_server_stats(self._h, C.byref(r)))
+        return {f: getattr(r, f) for f, _ in r._fields_}
+
+    def reset_stats(self) -> None:
+        check(lib().de_server_reset_stats(self._h))
+
+    def last_disparity(self, stream: int, W: int, H: int) -> np.ndarray:
+        out = np.empty((H, W), np.float32)
+        check(lib().de_server_last_disparity(self._h, int(stream), out.ctypes.data, W, H))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            check(lib().de_server_destroy(self._h))
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclasses.dataclass
+class StreamSpec:
+    W: int
+    H: int
+    D: int
+    fps: float = 30.0
+
+
+# The serving workload: 16 camera streams at 30 Hz, mixed 640x480 (D=64) and 848x480
+# (D=128), plus one 1280x720 at D=192.
+SERVING_STREAMS = ([StreamSpec(640, 480, 64)] * 8 + [StreamSpec(848, 480, 128)] * 7 +
+                   [StreamSpec(1280, 720, 192)])
+
+
+def make_frames(specs: Sequence[StreamSpec], frames_per_stream: int = 3, seed: int = 0):
+    """Pre-rendered seeded video frames per stream (the scene translates 1-3 px per
+    frame with fresh sensor noise); the simulation cycles through them."""
+    from .synth import Video
+    out = []
+    for s, spec in enumerate(specs):
+        v = Video(spec.W, spec.H, spec.D - 1, stream_id=s, seed=seed + 1)
+        out.append([v.frame(t) for t in range(frames_per_stream)])
+    return out
+
+
+def simulate(server: Server, specs: Sequence[StreamSpec], frames, duration_s: float = 3.0,
+             jitter_ms: float = 3.0, seed: int = 0) -> dict:
+    """Submit every stream's frames at its rate (period 1/fps plus Gaussian jitter of
+    sigma jitter_ms, random phase per stream) for duration_s, collect all results, and
+    report the server's latency percentiles and the achieved throughput."""
+    rng = np.random.default_rng(seed)
+    events = []
+    for s, spec in enumerate(specs):
+        t = rng.uniform(0, 1.0 / spec.fps)
+        k = 0
+        while t < duration_s:
+            events.append((t + rng.normal(0, jitter_ms / 1e3), s, k))
+            t += 1.0 / spec.fps
+            k += 1
+    events.sort()
+    tickets = []
+    done = []
+    errors = []
+
+    def collector():
+        while True:
+            item = pending.get()
+            if item is None:
+                return
+            try:
+                done.append(server.wait(item)["latency_ms"])
+            except Exception as e:  # noqa: BLE001 - reported below
+                errors.append(str(e))
+
+    import queue
+    pending = queue.Queue()
+    threads = [threading.Thread(target=collector) for _ in range(4)]
+    for th in threads:
+        th.start()
+    server.reset_stats()
+    t0 = time.perf_counter()
+    for at, s, k in events:
+        delay = at - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        p = frames[s][k % len(frames[s])]
+        tk = server.submit(s, p.left, p.right, specs[s].D)
+        tickets.append(tk)
+        pending.put(tk)
+    for _ in threads:
+        pending.put(None)
+    for th in threads:
+        th.join()
+    wall = time.perf_counter() - t0
+    st = server.stats()
+    return {"requests": len(events), "completed": int(st["completed"]),
+            "failed": int(st["failed"]) + len(errors), "wall_s": wall,
+            "pairs_per_s": st["completed"] / wall, "p50_ms": st["p50_ms"],
+            "p99_ms": st["p99_ms"], "max_ms": st["max_ms"],
+            "mean_batch": st["mean_batch"], "batches": int(st["batches"]),
+            "offered_pairs_per_s": len(events) / duration_s}

@@ -297,6 +297,49 @@ DE_API int de_dense_problem_dev(const uint8_t* L, const uint8_t* R, int W, int H
                                 int dmax, int hw, int hh, int64_t* ei, int64_t* ej, float* se,
                                 long long cap, void* workspace, size_t bytes, void* stream);
 
+/* ---- serving: many camera streams, continuous batching ------------------------
+ * Replaces the reference's one-frame-at-a-time live loop
+ * (core/tools/de_dense_cuda.cu:670-770).  A server owns a device: any thread submits
+ * a pair (host buffers, copied at submit) tagged with its camera stream and gets a
+ * ticket; a worker admits waiting pairs first come first served into lanes (a CUDA
+ * stream with a device arena of hbm_budget / lanes bytes, allocated once), as many
+ * as fit the arena and max_batch, and runs each lane's batch through the dense
+ * pipeline while the next lane fills.  Results equal the plain pipeline's bit for
+ * bit.  Each camera stream keeps its latest disparity maps on the device. */
+typedef struct de_server de_server;
+typedef struct de_server_cfg {
+  int device;
+  size_t hbm_budget;     /* device bytes for all lanes' arenas */
+  int max_batch;         /* pairs per launch */
+  int lanes;             /* batches in flight (CUDA streams) */
+} de_server_cfg;
+typedef struct de_server_stats {
+  unsigned long long completed, failed, batches;
+  double mean_batch;     /* pairs per launch */
+  double p50_ms, p99_ms, max_ms;   /* submit-to-result latency of completed requests */
+  size_t max_pending;
+} de_server_report;
+DE_API void de_server_cfg_default(de_server_cfg* cfg);
+DE_API int de_server_create(const de_cfg* cfg, const de_server_cfg* scfg, de_server** out);
+/* dmax 0 = cfg's.  Returns at once with a ticket. */
+DE_API int de_server_submit(de_server* sv, int stream, const uint8_t* L, const uint8_t* R,
+                            int W, int H, int dmax, unsigned long long* ticket);
+/* Blocks up to timeout_ms (DE_ERR_TIMEOUT leaves the request waitable), then copies
+ * the outputs (any may be NULL): disp/margin f32, conf u8, and the DEDD planes q4
+ * (int16 sixteenths of a pixel, -32768 where declined) and qconf; frees the ticket. */
+DE_API int de_server_wait(de_server* sv, unsigned long long ticket, int timeout_ms,
+                          float* disp, float* margin, uint8_t* conf, int16_t* q4,
+                          uint8_t* qconf, double* latency_ms);
+DE_API int de_server_stats(de_server* sv, de_server_report* out);
+DE_API int de_server_reset_stats(de_server* sv);
+/* The newest disparity map a stream has on the device (waits for it), W x H f32. */
+DE_API int de_server_last_disparity(de_server* sv, int stream, float* host, int W, int H);
+DE_API int de_server_destroy(de_server* sv);
+/* DEDD planes from a disparity (and optional confidence) plane on the device:
+ * core/tools/de_dense_cuda.cu:729-746. */
+DE_API int de_dedd_encode_dev(const float* disp, const uint8_t* conf, int W, int H,
+                              int16_t* q4, uint8_t* qconf, void* stream);
+
 /* ---- dense, host pointers, context-owned memory, synchronous ----------------- */
 
 typedef struct de_ctx de_ctx;

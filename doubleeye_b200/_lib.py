@@ -135,6 +135,10 @@ SIGNATURES = {
     "de_dense_problem_edges": (C.c_longlong, [C.c_int] * 6),
     "de_dense_problem_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, vp, vp, vp, C.c_longlong, vp, C.c_size_t, vp]),
+    "de_graph_create": (C.c_int, [C.POINTER(DeCfg), C.POINTER(DePair), C.c_int, vp,
+                                  C.c_size_t, C.POINTER(vp)]),
+    "de_graph_launch": (C.c_int, [vp, vp]),
+    "de_graph_destroy": (C.c_int, [vp]),
     "de_server_cfg_default": (None, [vp]),
     "de_server_create": (C.c_int, [C.POINTER(DeCfg), vp, C.POINTER(vp)]),
     "de_server_submit": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,

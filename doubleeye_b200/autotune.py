@@ -1,0 +1,134 @@
+"""Autotuner for the dense pipeline's launch shapes.
+
+The kernels leave the arithmetic fixed; these knobs only change how work is laid
+onto the GPU, so every setting gives bit-identical results:
+
+  rows_ctas_per_sm  resident row-kernel CTAs per SM (persistent grid size)
+  cols_kt           column-kernel tile shape: disparities per lane (0 = by batch size)
+  cols_stage_kb     column-kernel bulk-copy ring depth, KB per CTA
+  solve_threads     threads per row in the row solve (the BP schedule's width)
+
+``tune`` times a batch under a coordinate-descent search over these values (CUDA
+events, warm-up first) and returns the fastest setting; ``Tuner`` caches the choice
+per device and workload signature (pair shapes, disparity ranges, iterations) in a
+JSON file next to the library, so a workload is tuned once per machine.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+from . import _lib
+
+KNOBS = {
+    "rows_ctas_per_sm": [4, 8, 32],
+    "cols_kt": [0, 8, 16],
+    "cols_stage_kb": [16, 32, 64],
+    "solve_threads": [128, 256, 512],
+}
+CACHE = os.path.join(_lib.PKG, "_lib", "autotune.json")
+
+
+def current() -> dict:
+    return {k: _lib.get_param(k) for k in KNOBS}
+
+
+def apply(knobs: dict) -> None:
+    for k, v in knobs.items():
+        _lib.set_param(k, int(v))
+
+
+def signature(cfg, shapes) -> str:
+    """Workload key: sorted (W, H, D) multiset plus the iteration count."""
+    from collections import Counter
+    D0 = cfg.dmax - cfg.dmin + 1
+    norm = Counter((int(W), int(H), int(d) - cfg.dmin + 1 if d else D0) for W, H, d in shapes)
+    body = ",".join(f"{W}x{H}xD{D}*{n}" for (W, H, D), n in sorted(norm.items()))
+    return f"iters{cfg.iters}:lrc{cfg.lrc}:{body}"
+
+
+def _time(run, reps: int, warmup: int) -> float:
+    import torch
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        run()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def tune(run, reps: int = 3, warmup: int = 2, rounds: int = 2) -> tuple[dict, float]:
+    """Coordinate descent from the current setting: for each knob in turn keep the
+    fastest value, two rounds.  ``run`` enqueues one batch.  Leaves the best setting
+    applied and returns it with its time (ms per batch)."""
+    best = current()
+    apply(best)
+    best_ms = _time(run, reps, warmup)
+    for _ in range(rounds):
+        improved = False
+        for k, values in KNOBS.items():
+            for v in values:
+                if v == best[k]:
+                    continue
+                trial = dict(best, **{k: v})
+                apply(trial)
+                ms = _time(run, reps, warmup)
+                if ms < best_ms * 0.99:
+                    best, best_ms, improved = trial, ms, True
+            apply(best)
+        if not improved:
+            break
+    apply(best)
+    return best, best_ms
+
+
+class Tuner:
+    """Per-device, per-workload knob cache (JSON next to the library)."""
+
+    _lock = threading.Lock()
+
+    def __init__(self, path: str = CACHE):
+        self.path = path
+        self.table = {}
+        if os.path.exists(path):
+            try:
+                with open(path) as f:
+                    self.table = json.load(f)
+            except (OSError, ValueError):
+                self.table = {}
+
+    @staticmethod
+    def _device_key() -> str:
+        import torch
+        p = torch.cuda.get_device_properties(torch.cuda.current_device())
+        return f"{p.name}:{p.multi_processor_count}"
+
+    def lookup(self, sig: str):
+        return self.table.get(self._device_key(), {}).get(sig)
+
+    def record(self, sig: str, knobs: dict, ms: float) -> None:
+        with self._lock:
+            self.table.setdefault(self._device_key(), {})[sig] = dict(knobs, ms=ms)
+            try:
+                tmp = self.path + ".tmp"
+                with open(tmp, "w") as f:
+                    json.dump(self.table, f, indent=1, sort_keys=True)
+                os.replace(tmp, self.path)
+            except OSError:
+                pass
+
+    def ensure(self, sig: str, run) -> dict:
+        """The cached setting for ``sig`` (applied), tuning it first if absent."""
+        hit = self.lookup(sig)
+        if hit is None:
+            knobs, ms = tune(run)
+            self.record(sig, knobs, ms)
+            return knobs
+        knobs = {k: hit[k] for k in KNOBS}
+        apply(knobs)
+        return knobs

@@ -17,7 +17,7 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdoubleeye_b200.so")
 
-SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu", "de_serve.cu"]
+SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu", "de_serve.cu", "de_graph.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

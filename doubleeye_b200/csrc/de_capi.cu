@@ -228,7 +228,9 @@ int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
     for (int i = 0; i < b.n; ++i)
       DE_CUDA(cudaMemsetAsync(b.p[i].rkey, 0, size_t(b.p[i].W) * b.p[i].H * 4, s));
   std::vector<cudaEvent_t> grp;
-  const bool timed = g_timer.on;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(s, &cap);
+  const bool timed = g_timer.on && cap == cudaStreamCaptureStatusNone;
   if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_census(dc, b, s));
   if (timed) timer_mark(s, &grp);

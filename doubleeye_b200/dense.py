@@ -128,11 +128,24 @@ class DenseMatcher:
     caching allocator); ``match_into`` writes caller-provided outputs and allocates
     nothing."""
 
-    def __init__(self, cfg: Optional[DeCfg] = None, device: int = 0):
+    def __init__(self, cfg: Optional[DeCfg] = None, device: int = 0, autotune: bool = False):
         torch = _torch()
         self.cfg = cfg or Cfg()
         self.device = torch.device("cuda", device)
         self._ws = None
+        self._tuner = None
+        if autotune:
+            from .autotune import Tuner
+            self._tuner = Tuner()
+
+    def tune_for(self, items, stream=None) -> dict:
+        """Pick (or recall) the fastest launch shapes for this batch's workload and
+        apply them; results are unchanged by the choice."""
+        from .autotune import Tuner, signature
+        self._tuner = self._tuner or Tuner()
+        _, shapes = self._pairs(items)
+        return self._tuner.ensure(signature(self.cfg, shapes),
+                                  lambda: self._launch(items, stream))
 
     def workspace_bytes(self, shapes) -> int:
         arr = (DePair * len(shapes))()
@@ -161,20 +174,43 @@ class DenseMatcher:
     def match_into(self, items, stream=None) -> None:
         """items: list of (L, R, dmax or 0, outputs dict).  Enqueues one batched launch
         set on ``stream`` (default: current)."""
+        for L, R, _, _ in items:
+            if L.dtype != _torch().uint8 or L.device != self.device or not L.is_contiguous():
+                raise ValueError("images must be contiguous CUDA uint8 tensors on the device")
+        if self._tuner is not None:
+            self.tune_for(items, stream)
+        self._launch(items, stream)
+
+    def _launch(self, items, stream=None) -> None:
+        arr, shapes = self._pairs(items)
+        need = self.workspace_bytes(shapes)
+        ws = self._workspace(need)
+        check(lib().de_dense_dev(C.byref(self.cfg), arr, len(items), ws.data_ptr(), need,
+                                 _stream_handle(stream)))
+
+    def _pairs(self, items):
         arr = (DePair * len(items))()
         shapes = []
         for i, (L, R, dmax, out) in enumerate(items):
-            if L.dtype != _torch().uint8 or L.device != self.device or not L.is_contiguous():
-                raise ValueError("images must be contiguous CUDA uint8 tensors on the device")
             H, W = L.shape
             shapes.append((W, H, dmax))
             ptr = lambda k: out[k].data_ptr() if out.get(k) is not None else None  # noqa
             arr[i] = DePair(L.data_ptr(), R.data_ptr(), W, H, dmax, ptr("disp"),
                             ptr("margin"), ptr("conf"), ptr("cand"))
+        return arr, shapes
+
+    def capture(self, items) -> "CapturedBatch":
+        """Capture this batch's launch set (fixed buffers) as a CUDA graph; the
+        returned object's ``launch(stream)`` replays it, reading the input tensors as
+        they are at replay time.  Holds its own workspace."""
+        torch = _torch()
+        arr, shapes = self._pairs(items)
         need = self.workspace_bytes(shapes)
-        ws = self._workspace(need)
-        check(lib().de_dense_dev(C.byref(self.cfg), arr, len(items), ws.data_ptr(), need,
-                                 _stream_handle(stream)))
+        ws = torch.empty(max(need, 256), dtype=torch.uint8, device=self.device)
+        g = C.c_void_p()
+        check(lib().de_graph_create(C.byref(self.cfg), arr, len(items), ws.data_ptr(), need,
+                                    C.byref(g)))
+        return CapturedBatch(g, ws, items)
 
     def match(self, L, R, dmax: int = 0, cand: bool = False, stream=None) -> dict:
         out = self.new_outputs(*L.shape, cand=cand)
@@ -186,6 +222,28 @@ class DenseMatcher:
         self.match_into([(p[0], p[1], p[2] if len(p) > 2 else 0, o)
                          for p, o in zip(pairs, outs)], stream)
         return outs
+
+
+class CapturedBatch:
+    """A batch captured as a CUDA graph (``DenseMatcher.capture``)."""
+
+    def __init__(self, handle, workspace, items):
+        self._g = handle
+        self._keep = (workspace, items)      # buffers the graph reads and writes
+
+    def launch(self, stream=None) -> None:
+        check(lib().de_graph_launch(self._g, _stream_handle(stream)))
+
+    def close(self) -> None:
+        if self._g:
+            check(lib().de_graph_destroy(self._g))
+            self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # --------------------------------------------------------------------------------------

@@ -242,6 +242,18 @@ DE_API int de_match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
                               int cap, int* n_out, de_match_stats* stats, void* workspace,
                               size_t bytes, void* stream);
 
+/* ---- a batch captured as a CUDA graph ---------------------------------------- */
+/* Captures de_dense_dev(cfg, pairs, n, workspace) once; each de_graph_launch replays
+ * the whole batch (status reset + four kernels) as one launch on the given stream,
+ * reading the captured input buffers as they are at replay time.  The buffers and
+ * the workspace must outlive the graph.  Knobs set with de_set_param are those in
+ * force at capture. */
+typedef struct de_graph de_graph;
+DE_API int de_graph_create(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace,
+                           size_t bytes, de_graph** out);
+DE_API int de_graph_launch(de_graph* g, void* stream);
+DE_API int de_graph_destroy(de_graph* g);
+
 /* ---- the Python entry points: edge-list MASDA in double precision ------------ */
 
 /* masda_sparse (article/masda_stereo.py:453-492) on device edge lists: ei/ej int64

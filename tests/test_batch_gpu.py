@@ -1,0 +1,123 @@
+"""Batching: uneven pair sizes and disparity ranges in one launch set, the same set
+replayed from a captured CUDA graph, and the autotuner's launch-shape knobs, which
+must never change a result."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def de():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import doubleeye_b200 as de
+    from doubleeye_b200 import build
+    build.build()
+    return de
+
+
+def same(a, b):
+    a, b = a.cpu().numpy(), b.cpu().numpy()
+    if a.dtype == np.float32:
+        return bool(((a.view(np.uint32) == b.view(np.uint32)) | (np.isnan(a) & np.isnan(b))).all())
+    return bool((a == b).all())
+
+
+SHAPES = [(320, 240, 64), (640, 480, 128), (200, 96, 32), (848, 480, 128), (333, 211, 96),
+          (1280, 720, 256), (320, 240, 64)]
+
+
+@pytest.fixture(scope="module")
+def batch(de):
+    from doubleeye_b200 import synth
+    pairs = [synth.slanted_planes(W, H, D - 1, seed=k, tag="batch-gpu") for k, (W, H, D) in
+             enumerate(SHAPES)]
+    Ls = [torch.from_numpy(p.left).cuda() for p in pairs]
+    Rs = [torch.from_numpy(p.right).cuda() for p in pairs]
+    return pairs, Ls, Rs
+
+
+def run(de, m, Ls, Rs, cand=True):
+    outs = [m.new_outputs(*L.shape, cand=cand) for L in Ls]
+    m.match_into([(L, R, D, o) for L, R, (_, _, D), o in zip(Ls, Rs, SHAPES, outs)])
+    torch.cuda.synchronize()
+    return outs
+
+
+def test_mixed_batch_equals_one_pair_at_a_time(de, batch):
+    pairs, Ls, Rs = batch
+    m = de.DenseMatcher(de.Cfg(iters=8))
+    got = run(de, m, Ls, Rs)
+    for k, (L, R) in enumerate(zip(Ls, Rs)):
+        one = m.new_outputs(*L.shape, cand=True)
+        m.match_into([(L, R, SHAPES[k][2], one)])
+        torch.cuda.synchronize()
+        for key in ("disp", "margin", "conf", "cand"):
+            assert same(got[k][key], one[key]), (k, key)
+
+
+def test_graph_replay_matches_direct_launch(de, batch):
+    pairs, Ls, Rs = batch
+    m = de.DenseMatcher(de.Cfg(iters=8))
+    ref = run(de, m, Ls, Rs)
+    Lc = [L.clone() for L in Ls]
+    Rc = [R.clone() for R in Rs]
+    outs = [m.new_outputs(*L.shape, cand=True) for L in Lc]
+    g = m.capture([(L, R, D, o) for L, R, (_, _, D), o in zip(Lc, Rc, SHAPES, outs)])
+    for _ in range(2):
+        g.launch()
+        torch.cuda.synchronize()
+        for k in range(len(SHAPES)):
+            for key in ("disp", "margin", "conf", "cand"):
+                assert same(outs[k][key], ref[k][key]), (k, key)
+    # new frames in the captured input buffers: the replay matches a direct launch
+    for k in range(len(SHAPES)):
+        Lc[k].copy_(Rs[k])
+        Rc[k].copy_(Ls[k].roll(-3, dims=1))
+    g.launch()
+    direct = run(de, m, Lc, Rc)
+    for k in range(len(SHAPES)):
+        assert same(outs[k]["disp"], direct[k]["disp"]), k
+    g.close()
+
+
+@pytest.mark.parametrize("knob", ["rows_ctas_per_sm", "cols_kt", "cols_stage_kb",
+                                  "solve_threads"])
+def test_knobs_never_change_results(de, batch, knob):
+    from doubleeye_b200 import autotune
+    pairs, Ls, Rs = batch
+    m = de.DenseMatcher(de.Cfg(iters=4))
+    saved = autotune.current()
+    try:
+        ref = run(de, m, Ls, Rs)
+        for v in autotune.KNOBS[knob]:
+            autotune.apply(dict(saved, **{knob: v}))
+            got = run(de, m, Ls, Rs)
+            for k in range(len(SHAPES)):
+                for key in ("disp", "conf", "cand"):
+                    assert same(got[k][key], ref[k][key]), (knob, v, k, key)
+    finally:
+        autotune.apply(saved)
+
+
+def test_autotune_picks_and_caches(de, batch, tmp_path):
+    from doubleeye_b200 import autotune
+    pairs, Ls, Rs = batch
+    saved = autotune.current()
+    try:
+        m = de.DenseMatcher(de.Cfg(iters=4))
+        m._tuner = autotune.Tuner(str(tmp_path / "tune.json"))
+        items = [(L, R, D, m.new_outputs(*L.shape)) for L, R, (_, _, D) in zip(Ls, Rs, SHAPES)]
+        knobs = m.tune_for(items)
+        assert set(knobs) == set(autotune.KNOBS)
+        for k, v in knobs.items():
+            assert v in autotune.KNOBS[k] or v == saved[k]
+        again = autotune.Tuner(str(tmp_path / "tune.json"))
+        sig = autotune.signature(m.cfg, [(L.shape[1], L.shape[0], D)
+                                         for L, (_, _, D) in zip(Ls, SHAPES)])
+        assert again.lookup(sig) is not None
+    finally:
+        autotune.apply(saved)

@@ -231,6 +231,100 @@ def run_reference(args) -> None:
     print(json.dumps(out), flush=True)
 
 
+def c4_pairs(seed: int = 4):
+    """The uneven batch: 64 slots with sizes drawn uniformly (seed-fixed) from
+    {320x240, 640x480, 848x480, 1280x720, 1920x1080}, D in {64, 128, 256} matched to
+    size; two distinct seeded slanted-plane scenes per size, reused across slots (the
+    generator takes seconds per large scene on the host)."""
+    from doubleeye_b200 import synth
+    shapes = list(synth.BATCH_SHAPES.items())
+    rng = synth.rng_for("batch-draw", synth.BASE_SEED)
+    scenes = {}
+    out = []
+    for i in range(64):
+        (W, H), D = shapes[int(rng.integers(0, len(shapes)))]
+        k = (W, H, i % 2)
+        if k not in scenes:
+            scenes[k] = synth.slanted_planes(W, H, D - 1, seed=seed + len(scenes),
+                                             tag=f"c4:{W}x{H}")
+        out.append((scenes[k], D))
+    return out
+
+
+def run_c4(de, local: int, steps: int, warmup: int) -> dict:
+    """Batched uneven workload: one launch set for all 64 pairs (autotuned launch
+    shapes, CUDA-graph replay) against one launch set per pair."""
+    import torch
+    from doubleeye_b200 import autotune
+    pairs = c4_pairs()
+    cfg = de.Cfg(iters=ITERS)
+    m = de.DenseMatcher(cfg, device=local)
+    Ls = [torch.from_numpy(p.left).cuda() for p, _ in pairs]
+    Rs = [torch.from_numpy(p.right).cuda() for p, _ in pairs]
+    items = [(L, R, D, m.new_outputs(*L.shape)) for L, R, (_, D) in zip(Ls, Rs, pairs)]
+    saved = autotune.current()
+    knobs = m.tune_for(items)
+    evals = sum(float(L.numel()) * D for L, (_, D) in zip(Ls, pairs))
+
+    def timed(fn, reps):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    ms_batch = timed(lambda: m.match_into(items), steps)
+    g = m.capture(items)
+    ms_graph = timed(g.launch, steps)
+    g.close()
+    ms_plain = timed(lambda: [m.match_into([it]) for it in items], max(1, steps // 2))
+    autotune.apply(saved)
+    sizes = {}
+    for p, D in pairs:
+        key = f"{p.left.shape[1]}x{p.left.shape[0]}/D{D}"
+        sizes[key] = sizes.get(key, 0) + 1
+    return {"workload": "64 pairs, uneven sizes and D in one launch set", "sizes": sizes,
+            "pairs_per_s": 64 / (ms_batch / 1e3), "graph_pairs_per_s": 64 / (ms_graph / 1e3),
+            "plain_pairs_per_s": 64 / (ms_plain / 1e3),
+            "batch_over_plain": ms_plain / min(ms_batch, ms_graph),
+            "g_disp_evals_per_s": evals / (min(ms_batch, ms_graph) / 1e3) / 1e9,
+            "ms_per_batch": min(ms_batch, ms_graph), "knobs": knobs,
+            "data": "synthetic, 2 scenes per size reused across the 64 slots"}
+
+
+def run_c5(de, local: int) -> dict:
+    """Serving: 16 camera streams at 30 Hz (640x480 D=64 x8, 848x480 D=128 x7,
+    1280x720 D=192 x1, Gaussian arrival jitter sigma 3 ms), then the same streams
+    offered at 10x the rate to find the sustained throughput; the plain path is
+    one synchronous host-API call per pair over the same frames."""
+    from doubleeye_b200 import serve
+    specs = serve.SERVING_STREAMS
+    frames = serve.make_frames(specs, frames_per_stream=2)
+    out = {"streams": "16 at 30 Hz: 640x480/D64 x8, 848x480/D128 x7, 1280x720/D192 x1",
+           "outputs": "DEDD planes (Q4 disparity + confidence) per request"}
+    with serve.Server(de.Cfg(iters=ITERS), device=local, hbm_budget=24 << 30, max_batch=16,
+                      lanes=2) as sv:
+        serve.simulate(sv, specs, frames, duration_s=0.5)              # warm-up
+        out["at_30hz"] = serve.simulate(sv, specs, frames, duration_s=3.0)
+        fast = [serve.StreamSpec(s.W, s.H, s.D, fps=300.0) for s in specs]
+        out["at_300hz"] = serve.simulate(sv, fast, frames, duration_s=2.0)
+    t0 = time.perf_counter()
+    n = 0
+    for s, spec in enumerate(specs):
+        for p in frames[s]:
+            de.run_dense(p.left, p.right, de.Cfg(dmax=spec.D, iters=ITERS), want_cand=False,
+                         device=local)
+            n += 1
+    out["plain_pairs_per_s"] = n / (time.perf_counter() - t0)
+    out["served_over_plain"] = out["at_300hz"]["pairs_per_s"] / out["plain_pairs_per_s"]
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import doubleeye_b200 as de
@@ -288,12 +382,13 @@ def run_ours(args) -> None:
 
     # --- end to end through the public host API -----------------------------------
     host = [(p.left, p.right) for p in pairs]
+    res = None
     for _ in range(max(1, Wm // 2)):
-        res = de.run_dense_batch(host, cfg, device=local)
+        res = de.run_dense_batch(host, cfg, device=local, out=res)
     barrier(ws)
     t0 = time.perf_counter()
     for _ in range(K):
-        res = de.run_dense_batch(host, cfg, device=local)
+        res = de.run_dense_batch(host, cfg, device=local, out=res)
     e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
     filled = float(np.mean([np.isfinite(r.disp).mean() for r in res]))
 
@@ -332,6 +427,9 @@ def run_ours(args) -> None:
                        "h2d_bytes_per_step": B * 2 * WH,
                        "d2h_bytes_per_step": B * 9 * WH},
                "gpu_launches": 4 * K * ((B + 63) // 64)}
+        if ws == 1 and not args.no_extras:
+            out["batched_c4"] = run_c4(de, local, K, Wm)
+            out["serving_c5"] = run_c5(de, local)
         if ws == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline_sample()
         print(json.dumps(out), flush=True)
@@ -349,6 +447,8 @@ def main() -> None:
     ap.add_argument("--pairs-per-step", type=int, default=16)
     ap.add_argument("--ref-sample", type=int, default=2, help="pairs per reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched (C4) and serving (C5) sections")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

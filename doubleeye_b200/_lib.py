@@ -141,7 +141,7 @@ SIGNATURES = {
     "de_graph_destroy": (C.c_int, [vp]),
     "de_server_cfg_default": (None, [vp]),
     "de_server_create": (C.c_int, [C.POINTER(DeCfg), vp, C.POINTER(vp)]),
-    "de_server_submit": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int,
+    "de_server_submit": (C.c_int, [vp, C.c_int, vp, vp, C.c_int, C.c_int, C.c_int, C.c_uint,
                                    C.POINTER(C.c_ulonglong)]),
     "de_server_wait": (C.c_int, [vp, C.c_ulonglong, C.c_int, vp, vp, vp, vp, vp,
                                  C.POINTER(C.c_double)]),

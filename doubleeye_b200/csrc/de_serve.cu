@@ -85,6 +85,7 @@ namespace {
 struct Req {
   uint64_t ticket = 0;
   int stream = 0, W = 0, H = 0, dmax = 0;
+  unsigned planes = 0;                 // DE_PLANE_* the client will read
   std::vector<uint8_t> L, R;
   std::vector<float> disp, margin;
   std::vector<uint8_t> conf, qconf;
@@ -132,6 +133,7 @@ struct de_server {
   std::unordered_map<uint64_t, Req*> reqs;
   uint64_t next_ticket = 1;
   std::unordered_map<int, StreamState> streams;
+  std::vector<Req*> pool;              // finished requests kept with their buffers
   std::vector<double> lat;
   uint64_t batches = 0, batched_pairs = 0, completed = 0, failed = 0;
   size_t max_pending = 0;
@@ -271,16 +273,16 @@ void deliver(de_server* sv, Lane& l) {
     Req* r = l.batch[i];
     const Slot& s = l.slots[i];
     const size_t WH = size_t(r->W) * r->H;
-    r->disp.resize(WH);
-    r->margin.resize(WH);
-    r->conf.resize(WH);
-    r->q4.resize(WH);
-    r->qconf.resize(WH);
-    std::memcpy(r->disp.data(), l.pin + s.disp, WH * 4);
-    std::memcpy(r->margin.data(), l.pin + s.margin, WH * 4);
-    std::memcpy(r->conf.data(), l.pin + s.conf, WH);
-    std::memcpy(r->q4.data(), l.pin + s.q4, WH * 2);
-    std::memcpy(r->qconf.data(), l.pin + s.qconf, WH);
+    auto take = [&](unsigned bit, auto& v, size_t off, size_t esz) {
+      if (!(r->planes & bit)) return;
+      v.resize(WH);
+      std::memcpy(v.data(), l.pin + off, WH * esz);
+    };
+    take(DE_PLANE_DISP, r->disp, s.disp, 4);
+    take(DE_PLANE_MARGIN, r->margin, s.margin, 4);
+    take(DE_PLANE_CONF, r->conf, s.conf, 1);
+    take(DE_PLANE_Q4, r->q4, s.q4, 2);
+    take(DE_PLANE_QCONF, r->qconf, s.qconf, 1);
     r->status = status;
     r->t_done = t;
     if (status) {
@@ -289,10 +291,6 @@ void deliver(de_server* sv, Lane& l) {
       sv->lat.push_back(t - r->t_submit);
       ++sv->completed;
     }
-    r->L.clear();
-    r->L.shrink_to_fit();
-    r->R.clear();
-    r->R.shrink_to_fit();
   }
   l.batch.clear();
   l.busy = false;
@@ -436,7 +434,7 @@ int de_server_create(const de_cfg* cfg, const de_server_cfg* scfg, de_server** o
 }
 
 int de_server_submit(de_server* sv, int stream, const uint8_t* L, const uint8_t* R, int W,
-                     int H, int dmax, unsigned long long* ticket) {
+                     int H, int dmax, unsigned planes, unsigned long long* ticket) {
   if (!sv || !L || !R || !ticket) return de::set_error(DE_ERR_ARG, "NULL argument");
   de_pair probe{};
   probe.L = L;
@@ -446,14 +444,26 @@ int de_server_submit(de_server* sv, int stream, const uint8_t* L, const uint8_t*
   probe.dmax = dmax;
   size_t dummy = 0;
   if (int rc = de_dense_workspace_bytes(&sv->cfg, &probe, 1, &dummy)) return rc;
-  Req* r = new Req;
+  Req* r = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (!sv->pool.empty()) {
+      r = sv->pool.back();
+      sv->pool.pop_back();
+    }
+  }
+  if (!r) r = new Req;
+  r->planes = planes ? planes : DE_PLANE_ALL;
+  r->status = 1;
   r->stream = stream;
   r->W = W;
   r->H = H;
   r->dmax = dmax;
   const size_t WH = size_t(W) * H;
-  r->L.assign(L, L + WH);
-  r->R.assign(R, R + WH);
+  r->L.resize(WH);
+  r->R.resize(WH);
+  std::memcpy(r->L.data(), L, WH);
+  std::memcpy(r->R.data(), R, WH);
   r->t_submit = now_ms();
   {
     std::lock_guard<std::mutex> lk(sv->mu);
@@ -487,15 +497,16 @@ int de_server_wait(de_server* sv, unsigned long long ticket, int timeout_ms, flo
   const int status = r->status;
   if (status == 0) {
     const size_t WH = size_t(r->W) * r->H;
-    if (disp) std::memcpy(disp, r->disp.data(), WH * 4);
-    if (margin) std::memcpy(margin, r->margin.data(), WH * 4);
-    if (conf) std::memcpy(conf, r->conf.data(), WH);
-    if (q4) std::memcpy(q4, r->q4.data(), WH * 2);
-    if (qconf) std::memcpy(qconf, r->qconf.data(), WH);
+    const unsigned p = r->planes;
+    if (disp && (p & DE_PLANE_DISP)) std::memcpy(disp, r->disp.data(), WH * 4);
+    if (margin && (p & DE_PLANE_MARGIN)) std::memcpy(margin, r->margin.data(), WH * 4);
+    if (conf && (p & DE_PLANE_CONF)) std::memcpy(conf, r->conf.data(), WH);
+    if (q4 && (p & DE_PLANE_Q4)) std::memcpy(q4, r->q4.data(), WH * 2);
+    if (qconf && (p & DE_PLANE_QCONF)) std::memcpy(qconf, r->qconf.data(), WH);
     if (latency_ms) *latency_ms = r->t_done - r->t_submit;
   }
   sv->reqs.erase(it);
-  delete r;
+  if (sv->pool.size() < 256) sv->pool.push_back(r); else delete r;
   if (status) return de::set_error(status, "request failed (%d)", status);
   return DE_OK;
 }
@@ -567,6 +578,7 @@ int de_server_destroy(de_server* sv) {
       if (kv.second.ev[k]) cudaEventDestroy(kv.second.ev[k]);
     }
   for (auto& kv : sv->reqs) delete kv.second;
+  for (Req* r : sv->pool) delete r;
   delete sv;
   return DE_OK;
 }

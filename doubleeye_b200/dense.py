@@ -80,9 +80,12 @@ def run_dense(left, right, cfg: Optional[DeCfg] = None, *, want_cand: bool = Tru
 
 
 def run_dense_batch(pairs: Sequence, cfg: Optional[DeCfg] = None, *, want_cand=False,
-                    device: int = 0) -> list[DenseResult]:
+                    device: int = 0, out: Optional[Sequence[DenseResult]] = None
+                    ) -> list[DenseResult]:
     """Many pairs of any sizes in one batched launch set.  ``pairs`` holds
-    (left, right) or (left, right, dmax) tuples; dmax defaults to the cfg's."""
+    (left, right) or (left, right, dmax) tuples; dmax defaults to the cfg's.  ``out``
+    may pass the DenseResult arrays of an earlier call to be overwritten (no new host
+    allocation per call)."""
     cfg = cfg or Cfg()
     ctx = _Ctx.get(device)
     check(lib().de_ctx_set_cfg(ctx, C.byref(cfg)))
@@ -93,9 +96,13 @@ def run_dense_batch(pairs: Sequence, cfg: Optional[DeCfg] = None, *, want_cand=F
         if L.shape != R.shape:
             raise ValueError("left and right differ in shape")
         H, W = L.shape
-        res = DenseResult(np.empty((H, W), np.float32), np.empty((H, W), np.float32),
-                          np.empty((H, W), np.uint8),
-                          np.empty((6, H, W), np.float32) if want_cand else None)
+        if out is not None and out[i].disp.shape == (H, W) and \
+                (out[i].cand is not None or not want_cand):
+            res = out[i]
+        else:
+            res = DenseResult(np.empty((H, W), np.float32), np.empty((H, W), np.float32),
+                              np.empty((H, W), np.uint8),
+                              np.empty((6, H, W), np.float32) if want_cand else None)
         keep += [L, R]
         outs.append(res)
         arr[i] = DePair(L.ctypes.data, R.ctypes.data, W, H, int(pr[2]) if len(pr) > 2 else 0,

@@ -35,6 +35,11 @@ class DeServerReport(C.Structure):
                 ("max_pending", C.c_size_t)]
 
 
+PLANES = {"disp": 1, "margin": 2, "conf": 4, "q4": 8, "qconf": 16}
+PLANE_DTYPES = {"disp": np.float32, "margin": np.float32, "conf": np.uint8, "q4": np.int16,
+                "qconf": np.uint8}
+
+
 def _u8(a) -> np.ndarray:
     a = np.ascontiguousarray(a, np.uint8)
     if a.ndim != 2:
@@ -55,27 +60,32 @@ class Server:
         self._shape = {}
         self._mu = threading.Lock()
 
-    def submit(self, stream: int, L, R, dmax: int = 0) -> int:
+    def submit(self, stream: int, L, R, dmax: int = 0, planes=None) -> int:
+        """Queue a pair; ``planes`` names the outputs that will be read (default all:
+        disp, margin, conf, q4, qconf)."""
         L, R = _u8(L), _u8(R)
         H, W = L.shape
+        names = tuple(planes) if planes else tuple(PLANES)
+        mask = sum(PLANES[n] for n in names)
         t = C.c_ulonglong()
         check(lib().de_server_submit(self._h, int(stream), L.ctypes.data, R.ctypes.data, W, H,
-                                     int(dmax), C.byref(t)))
+                                     int(dmax), mask, C.byref(t)))
         with self._mu:
-            self._shape[t.value] = (H, W)
+            self._shape[t.value] = (H, W, names)
         return t.value
 
-    def wait(self, ticket: int, timeout_ms: int = 60000) -> dict:
+    def wait(self, ticket: int, timeout_ms: int = 60000, out: dict | None = None) -> dict:
+        """Block for a result; ``out`` may supply the arrays to fill (reused across
+        calls, no allocation)."""
         with self._mu:
-            H, W = self._shape[ticket]
-        out = dict(disp=np.empty((H, W), np.float32), margin=np.empty((H, W), np.float32),
-                   conf=np.empty((H, W), np.uint8), q4=np.empty((H, W), np.int16),
-                   qconf=np.empty((H, W), np.uint8))
+            H, W, names = self._shape[ticket]
+        if out is None or any(out.get(n) is None or out[n].shape != (H, W) for n in names):
+            out = {n: np.empty((H, W), PLANE_DTYPES[n]) for n in names}
+        ptr = lambda n: out[n].ctypes.data if n in names else None  # noqa: E731
         lat = C.c_double()
         check(lib().de_server_wait(self._h, C.c_ulonglong(ticket), int(timeout_ms),
-                                   out["disp"].ctypes.data, out["margin"].ctypes.data,
-                                   out["conf"].ctypes.data, out["q4"].ctypes.data,
-                                   out["qconf"].ctypes.data, C.byref(lat)))
+                                   ptr("disp"), ptr("margin"), ptr("conf"), ptr("q4"),
+                                   ptr("qconf"), C.byref(lat)))
         with self._mu:
             del self._shape[ticket]
         out["latency_ms"] = lat.value
@@ -140,8 +150,9 @@ def make_frames(specs: Sequence[StreamSpec], frames_per_stream: int = 3, seed: i
 def simulate(server: Server, specs: Sequence[StreamSpec], frames, duration_s: float = 3.0,
              jitter_ms: float = 3.0, seed: int = 0) -> dict:
     """Submit every stream's frames at its rate (period 1/fps plus Gaussian jitter of
-    sigma jitter_ms, random phase per stream) for duration_s, collect all results, and
-    report the server's latency percentiles and the achieved throughput."""
+    sigma jitter_ms, random phase per stream) for duration_s, collect all results (the
+    live path's DEDD planes: Q4 disparity and confidence), and report the server's
+    latency percentiles and the achieved throughput."""
     rng = np.random.default_rng(seed)
     events = []
     for s, spec in enumerate(specs):
@@ -157,12 +168,15 @@ def simulate(server: Server, specs: Sequence[StreamSpec], frames, duration_s: fl
     errors = []
 
     def collector():
+        bufs = {}
         while True:
             item = pending.get()
             if item is None:
                 return
+            tk, shape = item
             try:
-                done.append(server.wait(item)["latency_ms"])
+                bufs[shape] = server.wait(tk, out=bufs.get(shape))
+                done.append(bufs[shape]["latency_ms"])
             except Exception as e:  # noqa: BLE001 - reported below
                 errors.append(str(e))
 
@@ -178,9 +192,9 @@ def simulate(server: Server, specs: Sequence[StreamSpec], frames, duration_s: fl
         if delay > 0:
             time.sleep(delay)
         p = frames[s][k % len(frames[s])]
-        tk = server.submit(s, p.left, p.right, specs[s].D)
+        tk = server.submit(s, p.left, p.right, specs[s].D, planes=("q4", "qconf"))
         tickets.append(tk)
-        pending.put(tk)
+        pending.put((tk, p.left.shape))
     for _ in threads:
         pending.put(None)
     for th in threads:

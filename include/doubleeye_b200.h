@@ -333,9 +333,17 @@ typedef struct de_server_stats {
 } de_server_report;
 DE_API void de_server_cfg_default(de_server_cfg* cfg);
 DE_API int de_server_create(const de_cfg* cfg, const de_server_cfg* scfg, de_server** out);
-/* dmax 0 = cfg's.  Returns at once with a ticket. */
+/* Output planes a request will be asked for (the server copies only these). */
+#define DE_PLANE_DISP 1u
+#define DE_PLANE_MARGIN 2u
+#define DE_PLANE_CONF 4u
+#define DE_PLANE_Q4 8u
+#define DE_PLANE_QCONF 16u
+#define DE_PLANE_ALL 31u
+/* dmax 0 = cfg's; planes 0 = all.  Copies L and R, returns at once with a ticket. */
 DE_API int de_server_submit(de_server* sv, int stream, const uint8_t* L, const uint8_t* R,
-                            int W, int H, int dmax, unsigned long long* ticket);
+                            int W, int H, int dmax, unsigned planes,
+                            unsigned long long* ticket);
 /* Blocks up to timeout_ms (DE_ERR_TIMEOUT leaves the request waitable), then copies
  * the outputs (any may be NULL): disp/margin f32, conf u8, and the DEDD planes q4
  * (int16 sixteenths of a pixel, -32768 where declined) and qconf; frees the ticket. */

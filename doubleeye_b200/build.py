@@ -17,7 +17,10 @@ CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdoubleeye_b200.so")
 
-SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu", "de_serve.cu", "de_graph.cu"]
+SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu",
+           "de_serve.cu", "de_graph.cu"]
+TOOLS = os.path.join(PKG, "tools")
+CLI = os.path.join(OUT_DIR, "de_dense_gpu")      # the reference-compatible command line
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -56,8 +59,27 @@ def stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def build_cli(force: bool = False, verbose: bool = False) -> str:
+    """de_dense_gpu: a host-only C++ program over the C ABI (g++, rpath to the lib)."""
+    src = os.path.join(TOOLS, "de_dense_gpu.cpp")
+    hdr = os.path.join(os.path.dirname(PKG), "include", "doubleeye_b200.h")
+    if (not force and os.path.exists(CLI) and
+            os.path.getmtime(CLI) >= max(os.path.getmtime(src), os.path.getmtime(hdr),
+                                         os.path.getmtime(LIB))):
+        return CLI
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++17", "-Wall",
+           "-I", os.path.dirname(hdr), src, "-L", OUT_DIR, "-ldoubleeye_b200",
+           "-Wl,-rpath,$ORIGIN", "-o", CLI + ".tmp"]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(CLI + ".tmp", CLI)
+    return CLI
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not stale():
+        build_cli(False, verbose)
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
     tmp = LIB + ".tmp"
@@ -68,6 +90,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with open(LIB + ".cmd", "w") as f:
         f.write(_stamp())
     os.replace(tmp, LIB)
+    build_cli(True, verbose)
     return LIB
 
 

@@ -325,6 +325,34 @@ def run_c5(de, local: int) -> dict:
     return out
 
 
+def run_c3(de, local: int, steps: int, warmup: int) -> dict:
+    """The large configuration: 1500x1000, disparities 0-255, 12 BP iterations, thin
+    strips and low-texture regions; device-timed, one pair and four pairs a launch."""
+    import torch
+    from doubleeye_b200 import synth
+    p = synth.large_scene()
+    cfg = de.Cfg(dmax=256, iters=12)
+    m = de.DenseMatcher(cfg, device=local)
+    L = torch.from_numpy(p.left).cuda()
+    R = torch.from_numpy(p.right).cuda()
+    out = {"workload": "1500x1000 D=256 iters=12 (strips, low texture)"}
+    for B in (1, 4):
+        items = [(L, R, 0, m.new_outputs(1000, 1500)) for _ in range(B)]
+        for _ in range(warmup):
+            m.match_into(items)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            m.match_into(items)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[f"pairs_per_s_b{B}"] = B / (ms / 1e3)
+        out[f"g_disp_evals_per_s_b{B}"] = B * 1500 * 1000 * 256 / (ms / 1e3) / 1e9
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import doubleeye_b200 as de
@@ -428,6 +456,7 @@ def run_ours(args) -> None:
                        "d2h_bytes_per_step": B * 9 * WH},
                "gpu_launches": 4 * K * ((B + 63) // 64)}
         if ws == 1 and not args.no_extras:
+            out["large_c3"] = run_c3(de, local, max(3, K // 4), Wm)
             out["batched_c4"] = run_c4(de, local, K, Wm)
             out["serving_c5"] = run_c5(de, local)
         if ws == 1 and not args.no_cpu_baseline:

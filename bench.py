@@ -153,13 +153,8 @@ def barrier(ws):
 
 
 def max_over_ranks(x: float, ws: int) -> float:
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from doubleeye_b200.replicas import max_over_ranks as mor
+    return mor(x) if ws > 1 else x
 
 
 def cpu_baseline_sample(budget_s: float = 15.0, max_pairs: int = 400) -> dict:
@@ -361,7 +356,8 @@ def run_ours(args) -> None:
     build.build()
     ws, rank, local = dist_setup()
     B, K, Wm = args.pairs_per_step, args.steps, args.warmup
-    pairs = make_pairs(B, 1000 * rank)
+    from doubleeye_b200.replicas import rank_seed
+    pairs = make_pairs(B, rank_seed(rank))
     cfg = de.Cfg(dmax=D, iters=ITERS)
     m = de.DenseMatcher(cfg, device=local)
     Ls = [torch.from_numpy(p.left).cuda() for p in pairs]

@@ -52,6 +52,15 @@ ALG_BYTES = {
 }
 STAGES = ["census", "rows", "cols", "solve"]
 
+# Algorithmic 32-bit integer operations per pair (the arithmetic roof of the
+# integer stages; tensor cores do not apply).  Per disparity evaluation: rows =
+# census XOR 2 + POPC 2 + table 1 + |dI| 2 + table 1 + blend 3 (score, 11) + two
+# recursive-filter steps 2 x 5 + int16 pack/unpack 2 = 23; cols = two filter steps
+# 2 x 5 + top-2 key and insert 4 = 14.  Census: 48 compare-and-set per pixel per
+# image.  The solve is latency-bound and has no arithmetic roof here.
+ALG_INT_OPS = {"census": 2 * 48 * 2 * WH, "rows": 23 * E, "cols": 14 * E}
+INT_OPS_PER_CLK_PER_SM = 64          # 32-bit IADD/IMAD/shift/logic, per SM per clock
+
 
 def load_peaks() -> dict:
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
@@ -430,6 +439,16 @@ def run_ours(args) -> None:
             "alg_bytes_per_launch": alg,
             "pipeline_frac": ALG_BYTES["pipeline"] * B * K / (ms / 1e3) / 1e9
             / peaks["hbm_gbs"] / ws}
+    # the integer-arithmetic roof per stage at the clock sampled during the timed run
+    import torch
+    clk_mhz = clk.summary().get("sm_mhz") or 1965.0
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    int_peak = sms * INT_OPS_PER_CLK_PER_SM * clk_mhz * 1e6 / 1e12      # T ops/s
+    roof["int_roof"] = {
+        st: {"achieved_tops": ALG_INT_OPS[st] * B / (per_launch[st] / 1e3) / 1e12,
+             "peak_tops": int_peak,
+             "frac": ALG_INT_OPS[st] * B / (per_launch[st] / 1e3) / 1e12 / int_peak}
+        for st in ALG_INT_OPS}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": K,

@@ -104,12 +104,16 @@ SIGNATURES = {
     "de_ctx_set_cfg": (C.c_int, [vp, C.POINTER(DeCfg)]),
     "de_ctx_dense": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]),
     "de_ctx_dense_batch": (C.c_int, [vp, C.POINTER(DePair), C.c_int]),
+    "de_ctx_keypoints": (C.c_int, [vp, vp, C.c_int, C.c_int, C.POINTER(DeDetCfg), vp, vp, vp,
+                                   C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "de_census_at_dev": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int,
                                    vp, vp, vp]),
     "de_detect_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.POINTER(DeDetCfg),
                                             C.POINTER(C.c_size_t)]),
     "de_detect_fast_dev": (C.c_int, [vp, C.c_int, C.c_int, C.POINTER(DeDetCfg), vp, C.c_int,
                                      vp, vp, C.c_size_t, vp]),
+    "de_keypoint_readout_dev": (C.c_int, [vp, C.c_int, vp, vp, vp, C.c_int, C.c_int, vp,
+                                          C.c_int, vp, vp]),
     "de_match_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.POINTER(DeMatchCfg),
                                            C.POINTER(C.c_size_t)]),
     "de_match_masda_dev": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, C.c_int, vp,

@@ -641,6 +641,51 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   return DE_OK;
 }
 
+int de_ctx_keypoints(de_ctx* c, const uint8_t* L, int W, int H, const de_det_cfg* det,
+                     const float* disp, const float* margin, de_kp_disparity* out, int cap,
+                     int* n_out, int* n_detected) {
+  if (!c || !L || !det || !disp || !n_out || cap < 0 || (cap > 0 && !out))
+    return fail(DE_ERR_ARG, "bad arguments");
+  DE_CUDA(cudaSetDevice(c->device));
+  const size_t WH = size_t(W) * H;
+  const size_t ws = de::detect_ws_bytes(W, H, det);
+  const int kcap = 1 << 16;
+  // device block: L | disp | margin | keypoints | readout | counts
+  const size_t oL = 0, oD = align_up(oL + WH), oM = align_up(oD + WH * 4),
+               oK = align_up(oM + WH * 4), oR = align_up(oK + size_t(kcap) * 16),
+               oN = align_up(oR + size_t(kcap) * 16), end = align_up(oN + 16);
+  int rc;
+  if ((rc = grow_dev(&c->dws, &c->dws_cap, ws))) return rc;
+  if ((rc = grow_dev(&c->dio, &c->dio_cap, end))) return rc;
+  if ((rc = grow_host(&c->hio, &c->hio_cap, end))) return rc;
+  uint8_t* Hb = static_cast<uint8_t*>(c->hio);
+  uint8_t* Db = static_cast<uint8_t*>(c->dio);
+  std::memcpy(Hb + oL, L, WH);
+  std::memcpy(Hb + oD, disp, WH * 4);
+  if (margin) std::memcpy(Hb + oM, margin, WH * 4);
+  else std::memset(Hb + oM, 0, WH * 4);
+  DE_CUDA(cudaMemcpyAsync(Db, Hb, oK, cudaMemcpyHostToDevice, c->stream));
+  de_keypoint* kp = reinterpret_cast<de_keypoint*>(Db + oK);
+  int* counts = reinterpret_cast<int*>(Db + oN);
+  if ((rc = de::detect_fast_dev(Db + oL, W, H, det, kp, kcap, counts, c->dws, c->dws_cap,
+                                c->stream)))
+    return rc;
+  if ((rc = de::kp_readout_dev(kp, kcap, counts, reinterpret_cast<const float*>(Db + oD),
+                               reinterpret_cast<const float*>(Db + oM), W, H,
+                               reinterpret_cast<de_kp_disparity*>(Db + oR), kcap, counts + 1,
+                               c->stream)))
+    return rc;
+  DE_CUDA(cudaMemcpyAsync(Hb + oR, Db + oR, end - oR, cudaMemcpyDeviceToHost, c->stream));
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  int cnt[2];
+  std::memcpy(cnt, Hb + oN, sizeof(cnt));
+  if (cnt[0] < 0) return fail(DE_ERR_TIMEOUT, "keypoint suppression did not settle");
+  if (n_detected) *n_detected = cnt[0];
+  *n_out = cnt[1];
+  std::memcpy(out, Hb + oR, size_t(std::min(cnt[1], cap)) * sizeof(de_kp_disparity));
+  return DE_OK;
+}
+
 int de_ctx_dense(de_ctx* c, const uint8_t* L, const uint8_t* R, int W, int H, float* disp,
                  float* margin, uint8_t* conf, float* cand) {
   de_pair p{};

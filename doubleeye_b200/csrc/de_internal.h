@@ -98,5 +98,12 @@ void set_cols_stage_kb(int v);
 int get_cols_stage_kb();
 int get_cols_kt();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
+// Sparse path (de_sparse.cu), for the host-pointer context.
+size_t detect_ws_bytes(int W, int H, const de_det_cfg* c);
+int detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* c, de_keypoint* out,
+                    int cap, int* n_out, void* ws, size_t bytes, cudaStream_t s);
+int kp_readout_dev(const de_keypoint* kp, int n, const int* n_dev, const float* disp,
+                   const float* margin, int W, int H, de_kp_disparity* out, int cap,
+                   int* n_out, cudaStream_t s);
 
 }  // namespace de

@@ -836,6 +836,59 @@ __global__ void __launch_bounds__(1024, 1) k_match(MatchArgs a, MatchWs m) {
   }
 }
 
+
+// ---------------------------------------------------------------------------------
+// Keypoint read-out from a dense map (core/tools/de_dense_cuda.cu:866-899): each
+// keypoint looks up the disparity and margin at its rounded, clamped pixel; keypoints
+// where the map has no positive disparity are dropped; order is kept.  One CTA, an
+// ordered compaction in chunks of 1024.
+__global__ void __launch_bounds__(1024) k_kp_readout(const de_keypoint* kp, int n,
+                                                     const int* n_dev, const float* disp,
+                                                     const float* margin, int W, int H,
+                                                     de_kp_disparity* out, int cap,
+                                                     int* n_out) {
+  __shared__ int warp_cnt[32];
+  __shared__ int s_total;
+  const int cnt = n_dev ? max(0, min(n, *n_dev)) : n;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) s_total = 0;
+  __syncthreads();
+  for (int base = 0; base < cnt; base += 1024) {
+    const int i = base + threadIdx.x;
+    de_kp_disparity r{};
+    bool ok = false;
+    if (i < cnt) {
+      const de_keypoint k = kp[i];
+      const int x = min(max(int(k.x + 0.5f), 0), W - 1);
+      const int y = min(max(int(k.y + 0.5f), 0), H - 1);
+      const float d = disp[size_t(y) * W + x];
+      ok = d > 0.f;
+      r.x = k.x;
+      r.y = k.y;
+      r.disparity = d;
+      r.margin = margin ? margin[size_t(y) * W + x] : 0.f;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (lane == 0) warp_cnt[w] = __popc(b);
+    __syncthreads();
+    if (w == 0) {
+      int v = warp_cnt[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+      }
+      warp_cnt[lane] = v - warp_cnt[lane];        // exclusive
+    }
+    __syncthreads();
+    const int pos = s_total + warp_cnt[w] + __popc(b & ((1u << lane) - 1u));
+    if (ok && pos < cap) out[pos] = r;
+    __syncthreads();
+    if (threadIdx.x == 1023) s_total = pos + (ok ? 1 : 0);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *n_out = s_total;
+}
+
 int check_det(const de_det_cfg* c, int W, int H) {
   if (!c) return set_error(DE_ERR_ARG, "detector config is NULL");
   if (W < 16 || H < 16 || W > kMaxW || H > kMaxH)
@@ -914,6 +967,18 @@ int census_at_dev(const uint8_t* img, int W, int H, const de_keypoint* kp, int n
   return DE_OK;
 }
 
+int kp_readout_dev(const de_keypoint* kp, int n, const int* n_dev, const float* disp,
+                   const float* margin, int W, int H, de_kp_disparity* out, int cap,
+                   int* n_out, cudaStream_t s) {
+  if (n < 0 || cap < 0 || (n > 0 && (!kp || !disp)) || (cap > 0 && !out) || !n_out ||
+      W < 1 || H < 1)
+    return set_error(DE_ERR_ARG, "NULL keypoints, map or output, or bad size");
+  k_kp_readout<<<1, 1024, 0, s>>>(kp, n, n_dev, disp, margin, W, H, out, cap, n_out);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return set_error(DE_ERR_CUDA, "readout: %s", cudaGetErrorString(e));
+  return DE_OK;
+}
+
 int check_match_cfg(const de_match_cfg* c) {
   if (!c) return set_error(DE_ERR_ARG, "match config is NULL");
   if (c->max_candidates > 1024)
@@ -976,6 +1041,13 @@ int de_census_at_dev(const uint8_t* img, int W, int H, const de_keypoint* kp, in
                      void* stream) {
   return de::census_at_dev(img, W, H, kp, n, n_dev, hw, hh, desc, ok,
                            static_cast<cudaStream_t>(stream));
+}
+
+int de_keypoint_readout_dev(const de_keypoint* kp, int n, const int* n_dev,
+                            const float* disp, const float* margin, int W, int H,
+                            de_kp_disparity* out, int cap, int* n_out, void* stream) {
+  return de::kp_readout_dev(kp, n, n_dev, disp, margin, W, H, out, cap, n_out,
+                            static_cast<cudaStream_t>(stream));
 }
 
 int de_detect_workspace_bytes(int W, int H, const de_det_cfg* cfg, size_t* bytes) {

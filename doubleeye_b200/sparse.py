@@ -181,6 +181,29 @@ class SparseMatcher:
 
 # -- NumPy conveniences (one call each, synchronous) ------------------------------------
 
+KP_DISPARITY_DTYPE = np.dtype([("x", np.float32), ("y", np.float32),
+                               ("disparity", np.float32), ("margin", np.float32)])
+
+
+def dense_keypoints(left, disp, margin=None, det: Optional[DeDetCfg] = None,
+                    device: int = 0) -> tuple:
+    """The sparse feature set read out of a dense map (core/tools/de_dense_cuda.cu:
+    866-899): FAST keypoints of the left image that carry a positive disparity, with
+    the map's disparity and margin there.  Returns (records, number detected)."""
+    from .dense import _Ctx
+    L = np.ascontiguousarray(left, np.uint8)
+    H, W = L.shape
+    d = np.ascontiguousarray(disp, np.float32)
+    m = np.ascontiguousarray(margin, np.float32) if margin is not None else None
+    det = det or DetCfg()
+    cap = 1 << 16
+    out = np.zeros(cap, KP_DISPARITY_DTYPE)
+    n, nd = C.c_int(), C.c_int()
+    check(lib().de_ctx_keypoints(_Ctx.get(device), L.ctypes.data, W, H, C.byref(det),
+                                 d.ctypes.data, m.ctypes.data if m is not None else None,
+                                 out.ctypes.data, cap, C.byref(n), C.byref(nd)))
+    return out[:min(n.value, cap)].copy(), nd.value
+
 def detect_fast(img, det: Optional[DeDetCfg] = None, device: int = 0) -> np.ndarray:
     """detect_keypoints_fast on the GPU: (n, 4) float32 x, y, response, local_std."""
     sm = SparseMatcher(det=det, device=device)

@@ -9,7 +9,9 @@
 // --stream, "DEIR" frames (14-byte header + Y8) arrive on stdin, are paired by frame
 // number (stream 1 is the left camera), and each pair leaves on stdout as "DEDD"
 // (16-byte header, the left Y8, W*H int16 disparity in sixteenths of a pixel with
-// -32768 where declined, and W*H u8 confidence unless --no-confidence).
+// -32768 where declined, and W*H u8 confidence unless --no-confidence).  --keypoints
+// F.csv writes the sparse feature set read out of the dense map (x, y, disparity,
+// margin at FAST keypoints of the left image), as de_dense_cuda does.
 // Everything runs through the library's C ABI; flags of the reference's measured
 // negative paths (guided/box filters, --csct, --simd, --prior, --c2f, --topk != 2,
 // --dump-vol) are refused.
@@ -61,7 +63,8 @@ int usage(const char* argv0) {
                "       [--damping F] [--sigma-s F] [--sigma-r F] [--ad F] [--ad-trunc N]\n"
                "       [--min-margin F] [--min-ratio F] [--subpixel|--no-subpixel]\n"
                "       [--fit-eq|--fit-parabola] [--lrc] [--out F] [--out-conf F]\n"
-               "       [--frames N] [--device N] [--stream [--no-confidence]]\n",
+               "       [--keypoints F.csv] [--frames N] [--device N]\n"
+               "       [--stream [--no-confidence]]\n",
                argv0);
   return 2;
 }
@@ -74,7 +77,7 @@ int main(int argc, char** argv) {
   const int W = std::atoi(argv[3]), H = std::atoi(argv[4]);
   de_cfg cfg;
   de_cfg_default(&cfg);
-  std::string outp, confp;
+  std::string outp, confp, kpp;
   bool stream_mode = false, want_conf = true;
   int frames = 1, device = 0;
   for (int i = 5; i < argc; ++i) {
@@ -98,6 +101,7 @@ int main(int argc, char** argv) {
     else if (a == "--lrc") cfg.lrc = 1;
     else if (a == "--out" && has) outp = argv[++i];
     else if (a == "--out-conf" && has) confp = argv[++i];
+    else if (a == "--keypoints" && has) kpp = argv[++i];
     else if (a == "--frames" && has) frames = std::max(1, std::atoi(argv[++i]));
     else if (a == "--device" && has) device = std::atoi(argv[++i]);
     else if (a == "--stream") stream_mode = true;
@@ -229,6 +233,34 @@ int main(int argc, char** argv) {
   int rc = 0;
   if (!outp.empty() && !dump(outp, disp.data(), WH)) rc = 1;
   if (!confp.empty() && !dump(confp, cand.data(), WH * 6)) rc = 1;
+  if (!kpp.empty()) {
+    // the sparse feature set read out of the dense map (de_dense_cuda --keypoints)
+    de_det_cfg det;
+    de_det_cfg_default(&det);
+    std::vector<de_kp_disparity> kd(1 << 16);
+    int n = 0, detected = 0;
+    const double tk0 = now_ms();
+    if (de_ctx_keypoints(ctx, L.data(), W, H, &det, disp.data(), margin.data(), kd.data(),
+                         int(kd.size()), &n, &detected) != DE_OK) {
+      std::fprintf(stderr, "de_dense_gpu: %s\n", de_last_error());
+      de_ctx_destroy(ctx);
+      return 1;
+    }
+    const double tk1 = now_ms();
+    FILE* f = std::fopen(kpp.c_str(), "w");
+    if (!f) {
+      std::fprintf(stderr, "cannot write %s\n", kpp.c_str());
+      de_ctx_destroy(ctx);
+      return 1;
+    }
+    std::fprintf(f, "x,y,disparity,margin\n");
+    for (int k = 0; k < std::min(n, int(kd.size())); ++k)
+      std::fprintf(f, "%.2f,%.2f,%.4f,%.4f\n", kd[k].x, kd[k].y, kd[k].disparity,
+                   kd[k].margin);
+    std::fclose(f);
+    std::printf("keypoints: %d detected in %.1f ms, %d carried a disparity (%.1f%%) -> %s\n",
+                detected, tk1 - tk0, n, detected ? 100.0 * n / detected : 0.0, kpp.c_str());
+  }
   de_ctx_destroy(ctx);
   return rc;
 }

@@ -229,6 +229,15 @@ DE_API int de_detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg
                               de_keypoint* out, int cap, int* n_out, void* workspace,
                               size_t bytes, void* stream);
 
+/* The sparse feature set read out of a dense map (core/tools/de_dense_cuda.cu:866-899):
+ * for each keypoint, the disparity and margin at (int(x + 0.5), int(y + 0.5)) clamped
+ * to the image; keypoints whose disparity is not > 0 are dropped, order kept.
+ * Device pointers; n_dev (optional) limits n; margin may be NULL (reads 0). */
+typedef struct de_kp_disparity { float x, y, disparity, margin; } de_kp_disparity;
+DE_API int de_keypoint_readout_dev(const de_keypoint* kp, int n, const int* n_dev,
+                                   const float* disp, const float* margin, int W, int H,
+                                   de_kp_disparity* out, int cap, int* n_out, void* stream);
+
 /* match_masda (core/include/doubleeye/match.hpp:221-226, core/src/match.cpp:334-417)
  * on device keypoints and descriptors.  nl/nr are the array sizes; nl_dev/nr_dev,
  * if not NULL, are device counts that limit them (so a detector's output feeds
@@ -369,6 +378,13 @@ DE_API int de_ctx_set_cfg(de_ctx* ctx, const de_cfg* cfg);
 /* Host-buffer single pair: uploads L/R, runs de_dense_dev, downloads outputs. */
 DE_API int de_ctx_dense(de_ctx* ctx, const uint8_t* L, const uint8_t* R, int W, int H,
                         float* disp, float* margin, uint8_t* conf, float* cand);
+/* Keypoint read-out on host buffers (the --keypoints output of
+ * core/tools/de_dense_cuda.cu:866-899): detect keypoints in L (at most 65536), read
+ * the disparity and margin maps at them; *n_detected = keypoints found, *n_out = those
+ * with a disparity (at most cap written, in detection order). */
+DE_API int de_ctx_keypoints(de_ctx* ctx, const uint8_t* L, int W, int H, const de_det_cfg* det,
+                            const float* disp, const float* margin, de_kp_disparity* out,
+                            int cap, int* n_out, int* n_detected);
 /* The same for n host pairs in one batched launch. */
 DE_API int de_ctx_dense_batch(de_ctx* ctx, const de_pair* host_pairs, int n);
 

@@ -105,3 +105,29 @@ def test_stream_framing(cli, oracle, golden_dir):
         assert np.array_equal(q, want)
         conf = np.frombuffer(blk[16 + 3 * W * H:], np.uint8).reshape(H, W)
         assert (conf[~ok] == 0).all() and conf[ok].max() > 0
+
+
+@pytest.mark.gpu
+def test_keypoints_csv(cli, oracle, golden_dir, tmp_path):
+    needs_gpu()
+    from doubleeye_b200 import synth
+    p = synth.fronto_planes(424, 240, seed=12)
+    H, W = p.left.shape
+    p.left.tofile(tmp_path / "l.y8")
+    p.right.tofile(tmp_path / "r.y8")
+    r = run(cli, tmp_path / "l.y8", tmp_path / "r.y8", W, H, "--dmax", 64, "--iters", 4,
+            "--keypoints", tmp_path / "kp.csv")
+    assert r.returncode == 0, r.stderr
+    line = [ln for ln in r.stdout.decode().splitlines() if ln.startswith("keypoints:")][0]
+    rows = open(tmp_path / "kp.csv").read().splitlines()
+    assert rows[0] == "x,y,disparity,margin"
+    od, om, _ = oracle.dense(O.default_cfg(dmax=64, iters=4), p.left, p.right, want_cand=False)
+    kp = oracle.detect_fast(p.left, O.default_det_cfg())
+    want = []
+    for x, y, _, _ in kp:
+        xi = min(max(int(np.float32(x) + np.float32(0.5)), 0), W - 1)
+        yi = min(max(int(np.float32(y) + np.float32(0.5)), 0), H - 1)
+        if od[yi, xi] > 0:
+            want.append("%.2f,%.2f,%.4f,%.4f" % (x, y, od[yi, xi], om[yi, xi]))
+    assert rows[1:] == want
+    assert f"{len(kp)} detected" in line and f"{len(want)} carried" in line

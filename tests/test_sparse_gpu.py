@@ -219,3 +219,30 @@ def test_bad_arguments(sp):
         sp.match_masda(kp[:2], np.zeros(2, np.uint64), kp, np.zeros(16385, np.uint64))
     with pytest.raises(DeError):
         sp.census_at(np.zeros((32, 32), np.uint8), kp[:4], 5, 5)  # 11x11 > 64 bits
+
+
+def reference_readout(kp, disp, margin):
+    """core/tools/de_dense_cuda.cu:883-891 on NumPy arrays."""
+    H, W = disp.shape
+    rows = []
+    for x, y, _, _ in kp:
+        xi = min(max(int(np.float32(x) + np.float32(0.5)), 0), W - 1)
+        yi = min(max(int(np.float32(y) + np.float32(0.5)), 0), H - 1)
+        d = disp[yi, xi]
+        if not d > 0:
+            continue
+        rows.append((x, y, d, margin[yi, xi]))
+    return np.array(rows, np.float32).reshape(-1, 4)
+
+
+def test_keypoint_readout_from_dense_map(sp, oracle):
+    from oracle import oracle as O
+    p = c1(424, 240, seed=12)
+    d, m, _ = oracle.dense(O.default_cfg(dmax=64, iters=4), p.left, p.right, want_cand=False)
+    kp = oracle.detect_fast(p.left, O.default_det_cfg())
+    got, detected = sp.dense_keypoints(p.left, d, m)
+    want = reference_readout(kp, d, m)
+    assert detected == len(kp) and len(want) > 0.5 * len(kp)
+    assert got.view(np.float32).reshape(-1, 4).tobytes() == want.tobytes()
+    got0, _ = sp.dense_keypoints(p.left, d)                     # no margin plane: zeros
+    assert (got0["margin"] == 0).all() and len(got0) == len(got)

@@ -104,6 +104,12 @@ SIGNATURES = {
     "de_ctx_set_cfg": (C.c_int, [vp, C.POINTER(DeCfg)]),
     "de_ctx_dense": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]),
     "de_ctx_dense_batch": (C.c_int, [vp, C.POINTER(DePair), C.c_int]),
+    "de_ctx_dense_prior": (C.c_int, [vp, vp, vp, C.c_int, C.c_int, vp, C.c_int, vp, vp, vp,
+                                     vp]),
+    "de_dense_prior_workspace_bytes": (C.c_int, [C.POINTER(DeCfg), C.POINTER(DePair),
+                                                 C.POINTER(C.c_size_t)]),
+    "de_dense_prior_dev": (C.c_int, [C.POINTER(DeCfg), C.POINTER(DePair), vp, C.c_int, vp,
+                                     C.c_size_t, vp]),
     "de_ctx_keypoints": (C.c_int, [vp, vp, C.c_int, C.c_int, C.POINTER(DeDetCfg), vp, vp, vp,
                                    C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "de_census_at_dev": (C.c_int, [vp, C.c_int, C.c_int, vp, C.c_int, vp, C.c_int, C.c_int,

@@ -346,6 +346,48 @@ int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace
   return DE_OK;
 }
 
+int de_dense_prior_workspace_bytes(const de_cfg* cfg, const de_pair* pair, size_t* bytes) {
+  if (!bytes || !pair) return fail(DE_ERR_ARG, "NULL argument");
+  size_t ws = 0;
+  int rc = de_dense_workspace_bytes(cfg, pair, 1, &ws);
+  if (rc) return rc;
+  *bytes = ws + de::prior_ws_bytes(pair->W, pair->H, pair_D(*cfg, *pair));
+  return DE_OK;
+}
+
+int de_dense_prior_dev(const de_cfg* cfg, const de_pair* pair, const float* prior, int band,
+                       void* workspace, size_t ws_bytes, void* stream) {
+  size_t need = 0;
+  int rc = de_dense_prior_workspace_bytes(cfg, pair, &need);
+  if (rc) return rc;
+  if (!prior) return fail(DE_ERR_ARG, "prior is NULL");
+  if (band < 0 || band > DE_MAX_D) return fail(DE_ERR_ARG, "band %d outside 0..%d", band, DE_MAX_D);
+  if (cfg->census_hw != 3 || cfg->census_hh != 3)
+    return fail(DE_ERR_ARG, "the prior mask is the reference's 7x7-census path");
+  if (need > ws_bytes || !workspace)
+    return fail(DE_ERR_ARG, "workspace %zu bytes, need %zu", ws_bytes, need);
+  de_cfg c2 = *cfg;
+  c2.subpixel = 0;                    // as the reference tool does under a prior
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint8_t* ws = static_cast<uint8_t*>(workspace);
+  int* err = reinterpret_cast<int*>(ws);
+  DE_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  static de::Batch b;
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lk(mu);
+  fill_batch(c2, pair, 0, 1, ws + de::kStatusBytes, &b, err);
+  uint8_t* pws = ws + de::kStatusBytes +
+                 de::pair_workspace_bytes(pair->W, pair->H, pair_D(c2, *pair), c2.lrc != 0);
+  de::DevCfg dc;
+  de::make_dev_cfg(c2, &dc);
+  if (c2.lrc)
+    DE_CUDA(cudaMemsetAsync(b.p[0].rkey, 0, size_t(pair->W) * pair->H * 4, s));
+  DE_CUDA(de::launch_census(dc, b, s));
+  DE_CUDA(de::launch_prior(dc, b, prior, band, pws, s));
+  DE_CUDA(de::launch_solve(dc, b, false, s));
+  return DE_OK;
+}
+
 int de_census_dev(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
                   uint64_t* cl, uint64_t* cr, uint16_t* ax, uint16_t* ay, void* stream) {
   int rc = check_cfg(cfg);
@@ -683,6 +725,53 @@ int de_ctx_keypoints(de_ctx* c, const uint8_t* L, int W, int H, const de_det_cfg
   if (n_detected) *n_detected = cnt[0];
   *n_out = cnt[1];
   std::memcpy(out, Hb + oR, size_t(std::min(cnt[1], cap)) * sizeof(de_kp_disparity));
+  return DE_OK;
+}
+
+int de_ctx_dense_prior(de_ctx* c, const uint8_t* L, const uint8_t* R, int W, int H,
+                       const float* prior, int band, float* disp, float* margin,
+                       uint8_t* conf, float* cand) {
+  if (!c || !L || !R || !prior) return fail(DE_ERR_ARG, "bad arguments");
+  const size_t WH = size_t(W) * H;
+  for (size_t i = 0; i < WH; ++i)
+    if (!std::isfinite(prior[i]))
+      return fail(DE_ERR_ARG, "the prior has holes (non-finite values); fill them first");
+  DE_CUDA(cudaSetDevice(c->device));
+  de_pair p{};
+  p.L = L; p.R = R; p.W = W; p.H = H;
+  size_t ws = 0;
+  int rc = de_dense_prior_workspace_bytes(&c->cfg, &p, &ws);
+  if (rc) return rc;
+  const size_t oL = 0, oR = align_up(WH), oP = align_up(oR + WH), oD = align_up(oP + WH * 4),
+               oM = align_up(oD + WH * 4), oC = align_up(oM + WH * 4),
+               oX = align_up(oC + WH), end = align_up(oX + (cand ? WH * 24 : 0));
+  if ((rc = grow_dev(&c->dws, &c->dws_cap, ws))) return rc;
+  if ((rc = grow_dev(&c->dio, &c->dio_cap, end))) return rc;
+  if ((rc = grow_host(&c->hio, &c->hio_cap, end))) return rc;
+  uint8_t* Hb = static_cast<uint8_t*>(c->hio);
+  uint8_t* Db = static_cast<uint8_t*>(c->dio);
+  std::memcpy(Hb + oL, L, WH);
+  std::memcpy(Hb + oR, R, WH);
+  std::memcpy(Hb + oP, prior, WH * 4);
+  DE_CUDA(cudaMemcpyAsync(Db, Hb, oD, cudaMemcpyHostToDevice, c->stream));
+  de_pair dp{};
+  dp.L = Db + oL; dp.R = Db + oR; dp.W = W; dp.H = H;
+  dp.disp = reinterpret_cast<float*>(Db + oD);
+  dp.margin = reinterpret_cast<float*>(Db + oM);
+  dp.conf = Db + oC;
+  dp.cand = cand ? reinterpret_cast<float*>(Db + oX) : nullptr;
+  if ((rc = de_dense_prior_dev(&c->cfg, &dp, reinterpret_cast<const float*>(Db + oP), band,
+                               c->dws, c->dws_cap, c->stream)))
+    return rc;
+  DE_CUDA(cudaMemcpyAsync(Hb + oD, Db + oD, end - oD, cudaMemcpyDeviceToHost, c->stream));
+  int status = 0;
+  DE_CUDA(cudaMemcpyAsync(&status, c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  if (status) return fail(DE_ERR_TIMEOUT, "a bounded device wait ran out (status %d)", status);
+  if (disp) std::memcpy(disp, Hb + oD, WH * 4);
+  if (margin) std::memcpy(margin, Hb + oM, WH * 4);
+  if (conf) std::memcpy(conf, Hb + oC, WH);
+  if (cand) std::memcpy(cand, Hb + oX, WH * 24);
   return DE_OK;
 }
 

@@ -98,6 +98,10 @@ void set_cols_stage_kb(int v);
 int get_cols_stage_kb();
 int get_cols_kt();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
+// The prior-masked cost stage (de_prior.cu): one pair (b.p[0]) after its census.
+size_t prior_ws_bytes(int W, int H, int D);
+cudaError_t launch_prior(const DevCfg& cfg, const Batch& b, const float* prior, int band,
+                         void* ws, cudaStream_t s);
 // Sparse path (de_sparse.cu), for the host-pointer context.
 size_t detect_ws_bytes(int W, int H, const de_det_cfg* c);
 int detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* c, de_keypoint* out,

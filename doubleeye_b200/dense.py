@@ -112,6 +112,31 @@ def run_dense_batch(pairs: Sequence, cfg: Optional[DeCfg] = None, *, want_cand=F
     return outs
 
 
+def run_dense_prior(left, right, prior, cfg: Optional[DeCfg] = None, *, band: int = 2,
+                    want_cand: bool = True, device: int = 0) -> DenseResult:
+    """One pair with a disparity prior as the per-plane mask (the reference's --prior;
+    core/tools/de_dense.cpp:797-853): plane d is computed and offered only where the
+    prior's band [round(prior) - band, round(prior) + band] admits it.  ``prior`` is a
+    W x H float32 map without holes (a previous frame, a coarse pass); sub-pixel
+    refinement is off, as the reference sets it."""
+    cfg = cfg or Cfg()
+    ctx = _Ctx.get(device)
+    check(lib().de_ctx_set_cfg(ctx, C.byref(cfg)))
+    L, R = _u8(left), _u8(right)
+    H, W = L.shape
+    pr = np.ascontiguousarray(prior, np.float32)
+    if pr.shape != (H, W):
+        raise ValueError("the prior must be W x H")
+    res = DenseResult(np.empty((H, W), np.float32), np.empty((H, W), np.float32),
+                      np.empty((H, W), np.uint8),
+                      np.empty((6, H, W), np.float32) if want_cand else None)
+    check(lib().de_ctx_dense_prior(ctx, L.ctypes.data, R.ctypes.data, W, H, pr.ctypes.data,
+                                   int(band), res.disp.ctypes.data, res.margin.ctypes.data,
+                                   res.conf.ctypes.data,
+                                   res.cand.ctypes.data if want_cand else None))
+    return res
+
+
 # --------------------------------------------------------------------------------------
 # Device-tensor API (torch for device memory and streams; the work is the C ABI's)
 

@@ -13,8 +13,8 @@
 // F.csv writes the sparse feature set read out of the dense map (x, y, disparity,
 // margin at FAST keypoints of the left image), as de_dense_cuda does.
 // Everything runs through the library's C ABI; flags of the reference's measured
-// negative paths (guided/box filters, --csct, --simd, --prior, --c2f, --topk != 2,
-// --dump-vol) are refused.
+// negative paths (guided/box filters, --csct, --simd, --c2f, --topk != 2, --dump-vol)
+// are refused.  --prior F [--band N] runs the prior-masked path (sub-pixel off).
 
 #include <algorithm>
 #include <chrono>
@@ -63,7 +63,8 @@ int usage(const char* argv0) {
                "       [--damping F] [--sigma-s F] [--sigma-r F] [--ad F] [--ad-trunc N]\n"
                "       [--min-margin F] [--min-ratio F] [--subpixel|--no-subpixel]\n"
                "       [--fit-eq|--fit-parabola] [--lrc] [--out F] [--out-conf F]\n"
-               "       [--keypoints F.csv] [--frames N] [--device N]\n"
+               "       [--keypoints F.csv] [--prior F.f32 [--band N]] [--frames N]\n"
+               "       [--device N]\n"
                "       [--stream [--no-confidence]]\n",
                argv0);
   return 2;
@@ -77,7 +78,8 @@ int main(int argc, char** argv) {
   const int W = std::atoi(argv[3]), H = std::atoi(argv[4]);
   de_cfg cfg;
   de_cfg_default(&cfg);
-  std::string outp, confp, kpp;
+  std::string outp, confp, kpp, priorp;
+  int band = 2;
   bool stream_mode = false, want_conf = true;
   int frames = 1, device = 0;
   for (int i = 5; i < argc; ++i) {
@@ -102,6 +104,8 @@ int main(int argc, char** argv) {
     else if (a == "--out" && has) outp = argv[++i];
     else if (a == "--out-conf" && has) confp = argv[++i];
     else if (a == "--keypoints" && has) kpp = argv[++i];
+    else if (a == "--prior" && has) priorp = argv[++i];
+    else if (a == "--band" && has) band = std::atoi(argv[++i]);
     else if (a == "--frames" && has) frames = std::max(1, std::atoi(argv[++i]));
     else if (a == "--device" && has) device = std::atoi(argv[++i]);
     else if (a == "--stream") stream_mode = true;
@@ -204,13 +208,62 @@ int main(int argc, char** argv) {
     de_ctx_destroy(ctx);
     return 1;
   }
+  // --prior F: W*H floats, or (W/2)*(H/2) upsampled by nearest neighbour with the
+  // disparity doubled; holes are refused (core/tools/de_dense.cpp:1756-1813)
+  std::vector<float> prior;
+  if (!priorp.empty()) {
+    FILE* f = std::fopen(priorp.c_str(), "rb");
+    if (!f) {
+      std::fprintf(stderr, "cannot open prior %s\n", priorp.c_str());
+      de_ctx_destroy(ctx);
+      return 1;
+    }
+    std::fseek(f, 0, SEEK_END);
+    const size_t n = size_t(std::ftell(f)) / sizeof(float);
+    std::fseek(f, 0, SEEK_SET);
+    std::vector<float> raw(n);
+    const size_t got = std::fread(raw.data(), sizeof(float), n, f);
+    std::fclose(f);
+    const int W2 = W / 2, H2 = H / 2;
+    if (got != n || (n != WH && n != size_t(W2) * H2)) {
+      std::fprintf(stderr, "prior %s has %zu floats, expected %zu (full) or %zu (half)\n",
+                   priorp.c_str(), n, WH, size_t(W2) * H2);
+      de_ctx_destroy(ctx);
+      return 1;
+    }
+    prior.resize(WH);
+    if (n == WH) {
+      prior = raw;
+    } else {
+      for (int y = 0; y < H; ++y)
+        for (int x = 0; x < W; ++x)
+          prior[size_t(y) * W + x] =
+              2.f * raw[size_t(std::min(H2 - 1, y / 2)) * W2 + std::min(W2 - 1, x / 2)];
+    }
+    size_t holes = 0;
+    for (float v : prior) holes += std::isfinite(v) ? 0 : 1;
+    if (holes) {
+      std::fprintf(stderr, "prior has %zu holes of %zu; fill them first\n", holes, WH);
+      de_ctx_destroy(ctx);
+      return 1;
+    }
+    if (cfg.subpixel)
+      std::fprintf(stderr, "note: --prior disables sub-pixel (masked planes break the "
+                           "neighbour invariant); disparities are integer\n");
+  }
   std::vector<float> cand(confp.empty() ? 0 : WH * 6);
   de_stage_timing(1);
   double t_total = 0;
   for (int f = 0; f < frames; ++f) {
     const double t0 = now_ms();
-    if (de_ctx_dense(ctx, L.data(), R.data(), W, H, disp.data(), margin.data(), conf.data(),
-                     cand.empty() ? nullptr : cand.data()) != DE_OK) {
+    const int rc0 =
+        prior.empty()
+            ? de_ctx_dense(ctx, L.data(), R.data(), W, H, disp.data(), margin.data(),
+                           conf.data(), cand.empty() ? nullptr : cand.data())
+            : de_ctx_dense_prior(ctx, L.data(), R.data(), W, H, prior.data(), band,
+                                 disp.data(), margin.data(), conf.data(),
+                                 cand.empty() ? nullptr : cand.data());
+    if (rc0 != DE_OK) {
       std::fprintf(stderr, "de_dense_gpu: %s\n", de_last_error());
       de_ctx_destroy(ctx);
       return 1;

@@ -251,6 +251,18 @@ DE_API int de_match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
                               int cap, int* n_out, de_match_stats* stats, void* workspace,
                               size_t bytes, void* stream);
 
+/* ---- the disparity prior as a per-plane mask (--prior) ------------------------
+ * core/tools/de_dense.cpp:797-853,438-483,1166-1297 (run_dense with a prior, the
+ * --prior path of :1756-1813).  prior: W x H float32 disparities on the device (a
+ * previous frame, a coarse pass), no holes; plane d is computed only over the bounding
+ * box (padded by 8) of the pixels whose [round(prior) - band, round(prior) + band]
+ * contains d, and offered as a candidate only inside those pixels' row intervals.
+ * Sub-pixel refinement is off, as the reference's tool sets it.  One pair; 7x7 census. */
+DE_API int de_dense_prior_workspace_bytes(const de_cfg* cfg, const de_pair* pair,
+                                          size_t* bytes);
+DE_API int de_dense_prior_dev(const de_cfg* cfg, const de_pair* pair, const float* prior,
+                              int band, void* workspace, size_t bytes, void* stream);
+
 /* ---- a batch captured as a CUDA graph ---------------------------------------- */
 /* Captures de_dense_dev(cfg, pairs, n, workspace) once; each de_graph_launch replays
  * the whole batch (status reset + four kernels) as one launch on the given stream,
@@ -378,6 +390,11 @@ DE_API int de_ctx_set_cfg(de_ctx* ctx, const de_cfg* cfg);
 /* Host-buffer single pair: uploads L/R, runs de_dense_dev, downloads outputs. */
 DE_API int de_ctx_dense(de_ctx* ctx, const uint8_t* L, const uint8_t* R, int W, int H,
                         float* disp, float* margin, uint8_t* conf, float* cand);
+/* The prior path on host buffers; a prior with non-finite values is refused, as the
+ * reference refuses one with holes (core/tools/de_dense.cpp:1798-1805). */
+DE_API int de_ctx_dense_prior(de_ctx* ctx, const uint8_t* L, const uint8_t* R, int W, int H,
+                              const float* prior, int band, float* disp, float* margin,
+                              uint8_t* conf, float* cand);
 /* Keypoint read-out on host buffers (the --keypoints output of
  * core/tools/de_dense_cuda.cu:866-899): detect keypoints in L (at most 65536), read
  * the disparity and margin maps at them; *n_detected = keypoints found, *n_out = those

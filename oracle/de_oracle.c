@@ -425,19 +425,15 @@ static void solve_row_impl(const de_cfg* cfg, int W, const float* cs, const int*
 /* run_dense on the default path (core/tools/de_dense.cpp:738-1608) at one thread:
  * disp/margin f32[WH]; cand6 (may be NULL) = s1,s2,d1,d2,lrc,lrc2 planes with -1e30
  * in missing candidate slots, lrc NaN/-1e30 as the reference writes it. */
-void or_dense(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
-              float* disp, float* margin, float* cand6) {
+/* Row solves and the --out-conf planes from a cost stage's candidates. */
+static void finish_dense(const de_cfg* cfg, int W, int H, const float* cs, const int* cd,
+                         const int* cn, const int16_t* cnb, const int16_t* rk, float* disp,
+                         float* margin, float* cand6) {
   const size_t WH = (size_t)W * H;
-  float* cs = malloc(WH * 2 * sizeof(float));
-  int* cd = malloc(WH * 2 * sizeof(int));
-  int* cn = malloc(WH * sizeof(int));
-  int16_t* cnb = malloc(WH * 2 * sizeof(int16_t));
-  int16_t* rk = cfg->lrc ? malloc(WH * sizeof(int16_t)) : NULL;
   float* lrc2 = malloc(WH * sizeof(float));
-  or_cost_top2(cfg, L, R, W, H, cs, cd, cn, cnb, rk);
   for (int y = 0; y < H; ++y)
     or_solve_row(cfg, W, cs + (size_t)y * W * 2, cd + (size_t)y * W * 2, cn + (size_t)y * W,
-                 cfg->subpixel ? cnb + (size_t)y * W * 2 : NULL, disp + (size_t)y * W,
+                 (cfg->subpixel && cnb) ? cnb + (size_t)y * W * 2 : NULL, disp + (size_t)y * W,
                  margin + (size_t)y * W, lrc2 + (size_t)y * W);
   if (cand6) {
     for (size_t i = 0; i < WH * 6; ++i) cand6[i] = NEG_BIG;
@@ -463,7 +459,179 @@ void or_dense(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int 
           cand6[4 * WH + i] = r;
         }
   }
-  free(cs); free(cd); free(cn); free(cnb); free(rk); free(lrc2);
+  free(lrc2);
+}
+
+void or_dense(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+              float* disp, float* margin, float* cand6) {
+  const size_t WH = (size_t)W * H;
+  float* cs = malloc(WH * 2 * sizeof(float));
+  int* cd = malloc(WH * 2 * sizeof(int));
+  int* cn = malloc(WH * sizeof(int));
+  int16_t* cnb = malloc(WH * 2 * sizeof(int16_t));
+  int16_t* rk = cfg->lrc ? malloc(WH * sizeof(int16_t)) : NULL;
+  or_cost_top2(cfg, L, R, W, H, cs, cd, cn, cnb, rk);
+  finish_dense(cfg, W, H, cs, cd, cn, cnb, rk, disp, margin, cand6);
+  free(cs); free(cd); free(cn); free(cnb); free(rk);
+}
+
+/* ---- the disparity prior as a per-plane mask (--prior) ------------------------ */
+
+/* The recursive filter over a sub-rectangle, rows [y0, y1), columns [x0, x1):
+ * core/tools/de_dense.cpp:438-483.  The chains start at the rectangle's edges. */
+void or_filter_i16_rect(int16_t* C, const uint16_t* ax, const uint16_t* ay, int W, int y0,
+                        int y1, int x0, int x1) {
+  if (y1 - y0 < 1 || x1 - x0 < 2) return;
+  for (int y = y0; y < y1; ++y) {
+    int16_t* row = C + (size_t)y * W;
+    const uint16_t* a = ax + (size_t)y * W;
+    int32_t f = row[x0];
+    for (int x = x0 + 1; x < x1; ++x) {
+      const int32_t c = row[x];
+      f = c + (((int32_t)a[x] * (f - c) + (1 << 14)) >> 15);
+      row[x] = (int16_t)f;
+    }
+    f = row[x1 - 1];
+    for (int x = x1 - 2; x >= x0; --x) {
+      const int32_t c = row[x];
+      f = c + (((int32_t)a[x + 1] * (f - c) + (1 << 14)) >> 15);
+      row[x] = (int16_t)f;
+    }
+  }
+  for (int y = y0 + 1; y < y1; ++y) {
+    int16_t* cur = C + (size_t)y * W;
+    const int16_t* prv = C + (size_t)(y - 1) * W;
+    const uint16_t* a = ay + (size_t)y * W;
+    for (int x = x0; x < x1; ++x) {
+      const int32_t c = cur[x];
+      cur[x] = (int16_t)(c + (((int32_t)a[x] * (prv[x] - c) + (1 << 14)) >> 15));
+    }
+  }
+  for (int y = y1 - 2; y >= y0; --y) {
+    int16_t* cur = C + (size_t)y * W;
+    const int16_t* nxt = C + (size_t)(y + 1) * W;
+    const uint16_t* a = ay + (size_t)(y + 1) * W;
+    for (int x = x0; x < x1; ++x) {
+      const int32_t c = cur[x];
+      cur[x] = (int16_t)(c + (((int32_t)a[x] * (nxt[x] - c) + (1 << 14)) >> 15));
+    }
+  }
+}
+
+/* The mask of core/tools/de_dense.cpp:797-853: per row y and plane k the interval
+ * [mx0, mx1] of pixels whose band [round(prior) - band, round(prior) + band] (clamped
+ * to [dmin, dmax]) contains the plane, and per plane the bounding box of those. */
+void or_prior_mask(const de_cfg* cfg, const float* prior, int band, int W, int H,
+                   int16_t* mx0, int16_t* mx1, int* pylo, int* pyhi, int* pxlo, int* pxhi) {
+  const int D = cfg->dmax - cfg->dmin + 1;
+  for (size_t i = 0; i < (size_t)H * D; ++i) { mx0[i] = (int16_t)W; mx1[i] = -1; }
+  for (int k = 0; k < D; ++k) { pylo[k] = H; pyhi[k] = -1; pxlo[k] = W; pxhi[k] = -1; }
+  for (int y = 0; y < H; ++y) {
+    int16_t* r0 = mx0 + (size_t)y * D;
+    int16_t* r1 = mx1 + (size_t)y * D;
+    for (int x = 0; x < W; ++x) {
+      const int dc = (int)lroundf(prior[(size_t)y * W + x]);
+      const int klo = imax(cfg->dmin, dc - band) - cfg->dmin;
+      const int khi = imin(cfg->dmax, dc + band) - cfg->dmin;
+      for (int k = klo; k <= khi; ++k) {
+        if (x < r0[k]) r0[k] = (int16_t)x;
+        if (x > r1[k]) r1[k] = (int16_t)x;
+      }
+    }
+  }
+  for (int y = 0; y < H; ++y)
+    for (int k = 0; k < D; ++k) {
+      const int a = mx0[(size_t)y * D + k], b = mx1[(size_t)y * D + k];
+      if (b < a) continue;
+      if (y < pylo[k]) pylo[k] = y;
+      if (y > pyhi[k]) pyhi[k] = y;
+      if (a < pxlo[k]) pxlo[k] = a;
+      if (b > pxhi[k]) pxhi[k] = b;
+    }
+}
+
+/* Cost stage under the mask: core/tools/de_dense.cpp:1166-1297 with a prior.  A plane
+ * no pixel wants is skipped; otherwise its score is filtered over its bounding box
+ * padded by 8 (within the valid window) and inserted only inside the row intervals.
+ * Sub-pixel neighbours are not captured (the reference turns sub-pixel off here). */
+void or_cost_top2_prior(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                        const float* prior, int band, float* cs, int* cd, int* cn,
+                        int16_t* rbest_k) {
+  const size_t WH = (size_t)W * H;
+  const int D = cfg->dmax - cfg->dmin + 1;
+  const int hw = cfg->census_hw, hh = cfg->census_hh;
+  const int MPAD = 8;
+  uint64_t* cl = malloc(WH * sizeof(uint64_t));
+  uint64_t* cr = malloc(WH * sizeof(uint64_t));
+  uint16_t* ax = malloc(WH * sizeof(uint16_t));
+  uint16_t* ay = malloc(WH * sizeof(uint16_t));
+  int16_t* cur = malloc(WH * sizeof(int16_t));
+  int16_t *ts0 = malloc(WH * 2), *ts1 = malloc(WH * 2), *td0 = malloc(WH * 2),
+          *td1 = malloc(WH * 2), *trs = malloc(WH * 2);
+  int16_t* mx0 = malloc((size_t)H * D * 2);
+  int16_t* mx1 = malloc((size_t)H * D * 2);
+  int *pylo = malloc(D * sizeof(int)), *pyhi = malloc(D * sizeof(int)),
+      *pxlo = malloc(D * sizeof(int)), *pxhi = malloc(D * sizeof(int));
+  uint16_t lut[256];
+  or_census(L, W, H, hw, hh, cl);
+  or_census(R, W, H, hw, hh, cr);
+  or_rf_lut(cfg->sigma_s, cfg->sigma_r, lut);
+  or_rf_coeffs(L, W, H, lut, ax, ay);
+  or_prior_mask(cfg, prior, band, W, H, mx0, mx1, pylo, pyhi, pxlo, pxhi);
+  for (size_t i = 0; i < WH; ++i) {
+    ts0[i] = ts1[i] = -32768;
+    td0[i] = td1[i] = -1;
+    trs[i] = -32768;
+    if (rbest_k) rbest_k[i] = -1;
+  }
+  for (int k = 0; k < D; ++k) {
+    const int d = cfg->dmin + k;
+    if (pyhi[k] < pylo[k]) continue;
+    const int rylo = imax(hh, pylo[k] - MPAD), ryhi = imin(H - hh, pyhi[k] + 1 + MPAD);
+    const int rxlo = imax(hw + d, pxlo[k] - MPAD), rxhi = imin(W - hw, pxhi[k] + 1 + MPAD);
+    if (ryhi - rylo < 1 || rxhi - rxlo < 2) continue;
+    or_score_plane(cfg, L, R, cl, cr, W, H, k, cur);
+    or_filter_i16_rect(cur, ax, ay, W, rylo, ryhi, rxlo, rxhi);
+    for (int y = imax(rylo, pylo[k]); y < imin(ryhi, pyhi[k] + 1); ++y) {
+      const int xa = imax(rxlo, mx0[(size_t)y * D + k]);
+      const int xb = imin(rxhi, mx1[(size_t)y * D + k] + 1);
+      for (int x = xa; x < xb; ++x) {
+        const size_t i = (size_t)y * W + x;
+        const int16_t v = cur[i];
+        if (rbest_k && v > trs[i - d]) { trs[i - d] = v; rbest_k[i - d] = (int16_t)k; }
+        if (v <= ts1[i]) continue;
+        if (v > ts0[i]) { ts1[i] = ts0[i]; td1[i] = td0[i]; ts0[i] = v; td0[i] = (int16_t)k; }
+        else { ts1[i] = v; td1[i] = (int16_t)k; }
+      }
+    }
+  }
+  const float q = 1.f / (float)Q14;
+  for (size_t i = 0; i < WH; ++i) {
+    int n = 0;
+    cs[2 * i] = cs[2 * i + 1] = NEG_BIG;
+    cd[2 * i] = cd[2 * i + 1] = -1;
+    if (td0[i] >= 0) { cs[2 * i] = (float)ts0[i] * q; cd[2 * i] = td0[i]; n = 1; }
+    if (td1[i] >= 0) { cs[2 * i + 1] = (float)ts1[i] * q; cd[2 * i + 1] = td1[i]; n = 2; }
+    cn[i] = n;
+  }
+  free(cl); free(cr); free(ax); free(ay); free(cur); free(ts0); free(ts1); free(td0);
+  free(td1); free(trs); free(mx0); free(mx1); free(pylo); free(pyhi); free(pxlo); free(pxhi);
+}
+
+/* The dense pipeline with a full-resolution prior (run_dense with a prior and
+ * cfg.band = band; sub-pixel off, as the tool forces it). */
+void or_dense_prior(const de_cfg* cfg_in, const uint8_t* L, const uint8_t* R, int W, int H,
+                    const float* prior, int band, float* disp, float* margin, float* cand6) {
+  de_cfg cfg = *cfg_in;
+  cfg.subpixel = 0;
+  const size_t WH = (size_t)W * H;
+  float* cs = malloc(WH * 2 * sizeof(float));
+  int* cd = malloc(WH * 2 * sizeof(int));
+  int* cn = malloc(WH * sizeof(int));
+  int16_t* rk = cfg.lrc ? malloc(WH * sizeof(int16_t)) : NULL;
+  or_cost_top2_prior(&cfg, L, R, W, H, prior, band, cs, cd, cn, rk);
+  finish_dense(&cfg, W, H, cs, cd, cn, NULL, rk, disp, margin, cand6);
+  free(cs); free(cd); free(cn); free(rk);
 }
 
 /* confidence / confidence_u8, core/include/doubleeye/dense_solve.hpp:158-171. */

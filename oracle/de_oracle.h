@@ -47,6 +47,15 @@ void or_solve_row_debug(const de_cfg* cfg, int W, const float* cs, const int* cd
                         float* lrc2, float* best_out, int* target_out);
 void or_dense(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
               float* disp, float* margin, float* cand6);
+void or_filter_i16_rect(int16_t* C, const uint16_t* ax, const uint16_t* ay, int W, int y0,
+                        int y1, int x0, int x1);
+void or_prior_mask(const de_cfg* cfg, const float* prior, int band, int W, int H,
+                   int16_t* mx0, int16_t* mx1, int* pylo, int* pyhi, int* pxlo, int* pxhi);
+void or_cost_top2_prior(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                        const float* prior, int band, float* cs, int* cd, int* cn,
+                        int16_t* rbest_k);
+void or_dense_prior(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                    const float* prior, int band, float* disp, float* margin, float* cand6);
 float or_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol);
 unsigned or_confidence_u8(float s1, float s2, float lambda, float lrc, float lrc_tol);
 

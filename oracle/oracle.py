@@ -141,6 +141,8 @@ class Oracle:
         L.or_solve_row_debug.argtypes = [C.POINTER(DeCfg), C.c_int] + [C.c_void_p] * 9
         L.or_dense.argtypes = [C.POINTER(DeCfg), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                C.c_void_p, C.c_void_p, C.c_void_p]
+        L.or_dense_prior.argtypes = [C.POINTER(DeCfg), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                     C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.or_confidence.argtypes = [C.c_float] * 5
         L.or_confidence.restype = C.c_float
         L.or_confidence_u8.argtypes = [C.c_float] * 5
@@ -348,6 +350,19 @@ class Oracle:
                           margin.ctypes.data, cand.ctypes.data if cand is not None else None)
         return disp, margin, cand
 
+    def dense_prior(self, cfg: DeCfg, L, R, prior, band=2, want_cand: bool = True):
+        L = np.ascontiguousarray(L, np.uint8)
+        R = np.ascontiguousarray(R, np.uint8)
+        pr = np.ascontiguousarray(prior, np.float32)
+        H, W = L.shape
+        disp = np.zeros((H, W), np.float32)
+        margin = np.zeros((H, W), np.float32)
+        cand = np.zeros((6, H, W), np.float32) if want_cand else None
+        self.lib.or_dense_prior(C.byref(cfg), L.ctypes.data, R.ctypes.data, W, H,
+                                pr.ctypes.data, band, disp.ctypes.data, margin.ctypes.data,
+                                cand.ctypes.data if cand is not None else None)
+        return disp, margin, cand
+
     def confidence(self, s1, s2, lam, lrc=0.0, tol=1.0) -> float:
         return self.lib.or_confidence(s1, s2, lam, lrc, tol)
 
@@ -374,6 +389,9 @@ class Reference:
         L.ref_rf_filter_i16.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         L.ref_run_dense.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(DeCfg),
                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.ref_run_dense_prior.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                          C.POINTER(DeCfg), C.c_int, C.c_void_p, C.c_int,
+                                          C.c_void_p, C.c_void_p, C.c_void_p]
         L.ref_confidence.argtypes = [C.c_float] * 5
         L.ref_confidence.restype = C.c_float
         L.ref_confidence_u8.argtypes = [C.c_float] * 5
@@ -428,6 +446,20 @@ class Reference:
                                disp.ctypes.data, margin.ctypes.data,
                                cand.ctypes.data if cand is not None else None, t3.ctypes.data)
         return disp, margin, cand, t3
+
+    def dense_prior(self, cfg: DeCfg, L, R, prior, band=2, nthreads=1, want_cand=True):
+        L = np.ascontiguousarray(L, np.uint8)
+        R = np.ascontiguousarray(R, np.uint8)
+        pr = np.ascontiguousarray(prior, np.float32)
+        H, W = L.shape
+        disp = np.zeros((H, W), np.float32)
+        margin = np.zeros((H, W), np.float32)
+        cand = np.zeros((6, H, W), np.float32) if want_cand else None
+        self.lib.ref_run_dense_prior(L.ctypes.data, R.ctypes.data, W, H, C.byref(cfg), band,
+                                     pr.ctypes.data, nthreads, disp.ctypes.data,
+                                     margin.ctypes.data,
+                                     cand.ctypes.data if cand is not None else None)
+        return disp, margin, cand
 
     def confidence(self, s1, s2, lam, lrc=0.0, tol=1.0):
         return self.lib.ref_confidence(s1, s2, lam, lrc, tol)

@@ -91,6 +91,26 @@ void ref_run_dense(const uint8_t* L, const uint8_t* R, int W, int H, const de_cf
   if (t3) { t3[0] = T.census; t3[1] = T.cost; t3[2] = T.solve; }
 }
 
+// run_dense with a full-resolution disparity prior as the per-plane mask
+// (core/tools/de_dense.cpp:738-1608 with prior; cfg.band = band, sub-pixel off as the
+// tool forces it under --prior, :1824-1839).
+void ref_run_dense_prior(const uint8_t* L, const uint8_t* R, int W, int H, const de_cfg* c,
+                         int band, const float* prior, int nthreads, float* disp,
+                         float* margin, float* cand) {
+  const Image8 li = wrap(L, W, H), ri = wrap(R, W, H);
+  Cfg cfg = to_cfg(c);
+  cfg.band = band;
+  cfg.subpixel = false;
+  std::vector<float> pr(prior, prior + size_t(W) * H);
+  std::vector<float> d, m, cd;
+  LevelTimes T;
+  run_dense(li, ri, cfg, nthreads < 1 ? 1 : nthreads, pr, "", &d, &m, &T,
+            cand ? &cd : nullptr);
+  std::memcpy(disp, d.data(), d.size() * sizeof(float));
+  if (margin) std::memcpy(margin, m.data(), m.size() * sizeof(float));
+  if (cand) std::memcpy(cand, cd.data(), cd.size() * sizeof(float));
+}
+
 float ref_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol) {
   return confidence(s1, s2, lambda, lrc, lrc_tol);
 }

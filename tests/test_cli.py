@@ -131,3 +131,26 @@ def test_keypoints_csv(cli, oracle, golden_dir, tmp_path):
             want.append("%.2f,%.2f,%.4f,%.4f" % (x, y, od[yi, xi], om[yi, xi]))
     assert rows[1:] == want
     assert f"{len(kp)} detected" in line and f"{len(want)} carried" in line
+
+
+@pytest.mark.gpu
+def test_prior_flag(cli, oracle, tmp_path):
+    needs_gpu()
+    from doubleeye_b200 import synth
+    p = synth.slanted_planes(200, 120, 47, seed=5, tag="prior")
+    H, W = p.left.shape
+    p.left.tofile(tmp_path / "l.y8")
+    p.right.tofile(tmp_path / "r.y8")
+    half = np.full((H // 2, W // 2), 11.25, np.float32)     # half resolution: doubled
+    half.tofile(tmp_path / "p.f32")
+    r = run(cli, tmp_path / "l.y8", tmp_path / "r.y8", W, H, "--dmax", 48, "--iters", 8,
+            "--prior", tmp_path / "p.f32", "--band", 3, "--out", tmp_path / "d.f32")
+    assert r.returncode == 0, r.stderr
+    full = np.full((H, W), 22.5, np.float32)
+    d, _, _ = oracle.dense_prior(O.default_cfg(dmax=48, iters=8), p.left, p.right, full, 3)
+    assert np.fromfile(tmp_path / "d.f32", np.float32).tobytes() == d.tobytes()
+    bad = full.copy()
+    bad[3, 3] = np.nan
+    bad.tofile(tmp_path / "bad.f32")
+    r = run(cli, tmp_path / "l.y8", tmp_path / "r.y8", W, H, "--prior", tmp_path / "bad.f32")
+    assert r.returncode == 1 and b"holes" in r.stderr

@@ -5,7 +5,7 @@ onto the GPU, so every setting gives bit-identical results:
 
   rows_ctas_per_sm  resident row-kernel CTAs per SM (persistent grid size)
   cols_kt           column-kernel tile shape: disparities per lane (0 = by batch size)
-  cols_stage_kb     column-kernel bulk-copy ring depth, KB per CTA
+  cols_pf           column-kernel prefetch depth: image rows loaded ahead of use
   solve_threads     threads per row in the row solve (the BP schedule's width)
 
 ``tune`` times a batch under a coordinate-descent search over these values (CUDA
@@ -23,8 +23,8 @@ from . import _lib
 
 KNOBS = {
     "rows_ctas_per_sm": [4, 8, 32],
-    "cols_kt": [0, 8, 16],
-    "cols_stage_kb": [16, 32, 64],
+    "cols_kt": [0, 4, 8, 16],
+    "cols_pf": [4, 8],
     "solve_threads": [128, 256, 512],
 }
 CACHE = os.path.join(_lib.PKG, "_lib", "autotune.json")
@@ -125,7 +125,7 @@ class Tuner:
     def ensure(self, sig: str, run) -> dict:
         """The cached setting for ``sig`` (applied), tuning it first if absent."""
         hit = self.lookup(sig)
-        if hit is None:
+        if hit is None or any(k not in hit for k in KNOBS):    # absent, or older knob set
             knobs, ms = tune(run)
             self.record(sig, knobs, ms)
             return knobs

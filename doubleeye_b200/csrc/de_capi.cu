@@ -8,6 +8,7 @@
 #include <cstring>
 #include <algorithm>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -501,7 +502,7 @@ int de_set_param(const char* name, int value) {
   if (!name) return fail(DE_ERR_ARG, "name is NULL");
   if (!std::strcmp(name, "rows_ctas_per_sm")) { de::set_rows_ctas_per_sm(value); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { de::set_cols_kt(value); return DE_OK; }
-  if (!std::strcmp(name, "cols_stage_kb")) { de::set_cols_stage_kb(value); return DE_OK; }
+  if (!std::strcmp(name, "cols_pf")) { de::set_cols_pf(value); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { de::set_solve_threads(value); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
@@ -510,7 +511,7 @@ int de_get_param(const char* name, int* value) {
   if (!name || !value) return fail(DE_ERR_ARG, "NULL argument");
   if (!std::strcmp(name, "rows_ctas_per_sm")) { *value = de::get_rows_ctas_per_sm(); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { *value = de::get_cols_kt(); return DE_OK; }
-  if (!std::strcmp(name, "cols_stage_kb")) { *value = de::get_cols_stage_kb(); return DE_OK; }
+  if (!std::strcmp(name, "cols_pf")) { *value = de::get_cols_pf(); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { *value = de::get_solve_threads(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
@@ -542,6 +543,8 @@ struct de_ctx {
   de_cfg cfg;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy = nullptr;                       // uploads/downloads beside compute
+  cudaEvent_t ev_in = nullptr, ev_done = nullptr;
   void* dws = nullptr;        size_t dws_cap = 0;
   void* dio = nullptr;        size_t dio_cap = 0;    // device images + outputs
   void* hio = nullptr;        size_t hio_cap = 0;    // pinned mirror of dio
@@ -595,6 +598,45 @@ IoPlan io_plan(const de_pair* hp, int n) {
   return plan;
 }
 
+// Host memory the GPU can reach directly: pinned by cudaHostAlloc or registered.
+bool host_pinned(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();                                // clear the sticky-free error
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Copies between pageable and pinned host memory, split over a few threads when
+// there is enough to move (one core's memcpy is far below host memory bandwidth).
+struct HostCopy { void* dst; const void* src; size_t n; };
+void parallel_copy(const std::vector<HostCopy>& jobs) {
+  size_t total = 0;
+  for (const HostCopy& j : jobs) total += j.n;
+  const unsigned hc = std::thread::hardware_concurrency();
+  const int nt = int(std::min<size_t>({8, hc > 1 ? hc / 2 : 1, total >> 22}));
+  if (nt <= 1) {
+    for (const HostCopy& j : jobs) std::memcpy(j.dst, j.src, j.n);
+    return;
+  }
+  // cut every copy into pieces of about total / (4 nt) bytes, dealt round-robin
+  const size_t piece = std::max<size_t>(size_t(1) << 20, total / (4 * size_t(nt)));
+  std::vector<HostCopy> pieces;
+  for (const HostCopy& j : jobs)
+    for (size_t o = 0; o < j.n; o += piece)
+      pieces.push_back({static_cast<uint8_t*>(j.dst) + o, static_cast<const uint8_t*>(j.src) + o,
+                        std::min(piece, j.n - o)});
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; ++t)
+    th.emplace_back([&pieces, t, nt] {
+      for (size_t k = t; k < pieces.size(); k += nt)
+        std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
+    });
+  for (size_t k = 0; k < pieces.size(); k += nt) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
+  for (std::thread& t : th) t.join();
+}
+
 }  // namespace
 
 extern "C" {
@@ -611,7 +653,13 @@ int de_ctx_create(const de_cfg* cfg, int device, de_ctx** out) {
   c->cfg = *cfg;
   c->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-  if (e != cudaSuccess) { delete c; return cuda_fail(e, "cudaStreamCreate"); }
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    de_ctx_destroy(c);
+    return cuda_fail(e, "creating the context's streams and events");
+  }
   *out = c;
   return DE_OK;
 }
@@ -620,9 +668,13 @@ int de_ctx_destroy(de_ctx* c) {
   if (!c) return DE_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->copy) cudaStreamSynchronize(c->copy);
   if (c->dws) cudaFree(c->dws);
   if (c->dio) cudaFree(c->dio);
   if (c->hio) cudaFreeHost(c->hio);
+  if (c->ev_in) cudaEventDestroy(c->ev_in);
+  if (c->ev_done) cudaEventDestroy(c->ev_done);
+  if (c->copy) cudaStreamDestroy(c->copy);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return DE_OK;
@@ -646,15 +698,29 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   const IoPlan plan = io_plan(hp, n);
   if ((rc = grow_dev(&c->dws, &c->dws_cap, ws))) return rc;
   if ((rc = grow_dev(&c->dio, &c->dio_cap, plan.end))) return rc;
-  if ((rc = grow_host(&c->hio, &c->hio_cap, plan.end))) return rc;
+  if ((rc = grow_host(&c->hio, &c->hio_cap, plan.end + kAlign))) return rc;
   uint8_t* Hb = static_cast<uint8_t*>(c->hio);
   uint8_t* Db = static_cast<uint8_t*>(c->dio);
+  int* hstat = reinterpret_cast<int*>(Hb + plan.end);   // pinned: one status word a chunk
+  hstat[0] = hstat[1] = 0;
+  // Each host buffer moves by DMA straight from or to the caller's memory when that
+  // memory is pinned, else through the context's pinned mirror at the same offset.
+  struct Io { void* host; size_t off, bytes; bool pinned; int pair; };
+  std::vector<Io> ins, outs;
   std::vector<de_pair> dp(n);
+  size_t out_bytes = 0;
   for (int i = 0; i < n; ++i) {
     const IoLayout& l = plan.p[i];
     const size_t WH = size_t(hp[i].W) * hp[i].H;
-    std::memcpy(Hb + l.L, hp[i].L, WH);
-    std::memcpy(Hb + l.R, hp[i].R, WH);
+    ins.push_back({const_cast<uint8_t*>(hp[i].L), l.L, WH, host_pinned(hp[i].L), i});
+    ins.push_back({const_cast<uint8_t*>(hp[i].R), l.R, WH, host_pinned(hp[i].R), i});
+    auto out = [&](void* h, size_t off, size_t bytes) {
+      if (h) { outs.push_back({h, off, bytes, host_pinned(h), i}); out_bytes += bytes; }
+    };
+    out(hp[i].disp, l.disp, WH * 4);
+    out(hp[i].margin, l.margin, WH * 4);
+    out(hp[i].conf, l.conf, WH);
+    out(hp[i].cand, l.cand, WH * 24);
     dp[i] = hp[i];
     dp[i].L = Db + l.L;
     dp[i].R = Db + l.R;
@@ -663,23 +729,52 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
     dp[i].conf = hp[i].conf ? Db + l.conf : nullptr;
     dp[i].cand = hp[i].cand ? reinterpret_cast<float*>(Db + l.cand) : nullptr;
   }
-  DE_CUDA(cudaMemcpyAsync(Db, Hb, plan.in_end, cudaMemcpyHostToDevice, c->stream));
-  if ((rc = de_dense_dev(&c->cfg, dp.data(), n, c->dws, c->dws_cap, c->stream))) return rc;
-  if (plan.end > plan.out_begin)
-    DE_CUDA(cudaMemcpyAsync(Hb + plan.out_begin, Db + plan.out_begin,
-                            plan.end - plan.out_begin, cudaMemcpyDeviceToHost, c->stream));
-  int status = 0;
-  DE_CUDA(cudaMemcpyAsync(&status, c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  DE_CUDA(cudaStreamSynchronize(c->stream));
+  // Two chunks when there is enough to move: the second chunk's upload and the first
+  // chunk's download run on the copy stream while the other chunk computes, so only
+  // the first upload and the (smaller) second download are not hidden.
+  const int n1 = (n >= 4 && out_bytes >= (size_t(8) << 20)) ? (3 * n + 3) / 4 : n;
+  std::vector<HostCopy> jobs;
+  for (const Io& io : ins)
+    if (!io.pinned) jobs.push_back({Hb + io.off, io.host, io.bytes});
+  parallel_copy(jobs);
+  auto move = [&](const Io& io, bool up, cudaStream_t st) -> cudaError_t {
+    void* h = io.pinned ? io.host : Hb + io.off;
+    return up ? cudaMemcpyAsync(Db + io.off, h, io.bytes, cudaMemcpyHostToDevice, st)
+              : cudaMemcpyAsync(h, Db + io.off, io.bytes, cudaMemcpyDeviceToHost, st);
+  };
+  auto enqueue = [&]() -> int {
+    int r;
+    for (const Io& io : ins) DE_CUDA(move(io, true, io.pair < n1 ? c->stream : c->copy));
+    if (n1 < n) DE_CUDA(cudaEventRecord(c->ev_in, c->copy));
+    if ((r = de_dense_dev(&c->cfg, dp.data(), n1, c->dws, c->dws_cap, c->stream))) return r;
+    DE_CUDA(cudaMemcpyAsync(&hstat[0], c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    if (n1 < n) {
+      DE_CUDA(cudaEventRecord(c->ev_done, c->stream));
+      DE_CUDA(cudaStreamWaitEvent(c->copy, c->ev_done, 0));
+      for (const Io& io : outs)
+        if (io.pair < n1) DE_CUDA(move(io, false, c->copy));
+      DE_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in, 0));
+      if ((r = de_dense_dev(&c->cfg, dp.data() + n1, n - n1, c->dws, c->dws_cap, c->stream)))
+        return r;
+      DE_CUDA(cudaMemcpyAsync(&hstat[1], c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    }
+    for (const Io& io : outs)
+      if (io.pair >= n1 || n1 == n) DE_CUDA(move(io, false, c->stream));
+    return DE_OK;
+  };
+  // whatever was enqueued finishes before the call returns, on success or not
+  rc = enqueue();
+  const cudaError_t e1 = cudaStreamSynchronize(c->stream);
+  const cudaError_t e2 = cudaStreamSynchronize(c->copy);
+  if (rc) return rc;
+  if (e1 != cudaSuccess) return cuda_fail(e1, "cudaStreamSynchronize");
+  if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamSynchronize");
+  const int status = hstat[0] ? hstat[0] : hstat[1];
   if (status) return fail(DE_ERR_TIMEOUT, "a bounded device wait ran out (status %d)", status);
-  for (int i = 0; i < n; ++i) {
-    const IoLayout& l = plan.p[i];
-    const size_t WH = size_t(hp[i].W) * hp[i].H;
-    if (hp[i].disp) std::memcpy(hp[i].disp, Hb + l.disp, WH * 4);
-    if (hp[i].margin) std::memcpy(hp[i].margin, Hb + l.margin, WH * 4);
-    if (hp[i].conf) std::memcpy(hp[i].conf, Hb + l.conf, WH);
-    if (hp[i].cand) std::memcpy(hp[i].cand, Hb + l.cand, WH * 24);
-  }
+  jobs.clear();
+  for (const Io& io : outs)
+    if (!io.pinned) jobs.push_back({io.host, Hb + io.off, io.bytes});
+  parallel_copy(jobs);
   return DE_OK;
 }
 

@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "de_internal.h"
@@ -54,6 +55,8 @@ __device__ __forceinline__ int find_pair(const int* prefix, int n, int item) {
 __device__ __forceinline__ int32_t rf_step(int32_t c, int32_t f, int32_t a) {
   return c + ((a * (f - c) + (1 << 14)) >> 15);
 }
+
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 __device__ __forceinline__ uint32_t pack2(int32_t lo, int32_t hi) {
   return (uint32_t(uint16_t(lo))) | (uint32_t(hi) << 16);
@@ -449,18 +452,6 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
 }
 
 // ---------------------------------------------------------------------------------
-// k_cols: vertical forward (in place), vertical backward + top-2 + neighbours.
-// Vertical passes: core/tools/de_dense.cpp:490-507.  Top-2 semantics: :1276-1292
-// (ascending k, strictly greater, ties keep the smaller k), sub-pixel neighbour
-// capture :1276-1285.
-//
-// A column is a group of TPC = Dpad/KT lanes (padded to TPCP, a power of two);
-// lane s of the group owns disparities [s*KT, s*KT + KT) as int16 pairs, so one row
-// of one column is 2*Dpad contiguous bytes read with 128-bit loads, and adjacent
-// columns are adjacent in memory.  The top-2 key (v + 32768) << 8 | (255 - k) is
-// unique per k, so the strictly-greater insertion is three unsigned min/max, the
-// merge across lanes is four, and any merge order gives the sequential scan's
-// answer.  The winner's neighbour costs are read back from a per-warp row buffer.
 __device__ __forceinline__ int32_t sx16(uint32_t v) {     // sign-extended low half
   return int32_t(int16_t(uint16_t(v & 0xFFFFu)));
 }
@@ -469,29 +460,67 @@ __device__ __forceinline__ uint32_t pk16(int32_t lo, int32_t hi) {
   return __byte_perm(uint32_t(lo), uint32_t(hi), 0x5410);
 }
 
-template <int KT, int TPCP>
-__global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b, int nstages) {
-  static_assert(KT % 8 == 0 && TPCP >= 1 && TPCP <= 32, "shape");
-  constexpr int NV = KT / 8;                         // 128-bit vectors per row per lane
+// k_cols: vertical forward (in place), vertical backward + top-2 + neighbours.
+// Vertical passes: core/tools/de_dense.cpp:490-507.  Top-2 semantics: :1276-1292
+// (ascending k, strictly greater, ties keep the smaller k), sub-pixel neighbour
+// capture :1276-1285.
+//
+// A column is a group of TPC = Dpad/KT lanes (padded to TPCP, a power of two);
+// lane s of the group owns disparities [s*KT, s*KT + KT) as int16 pairs, so one row
+// of one column is 2*Dpad contiguous bytes, and adjacent columns are adjacent in
+// memory.  The top-2 key (v + 32768) << 8 | (255 - k) is unique per k, so the
+// strictly-greater insertion is three unsigned min/max, the merge across lanes is
+// four, and any merge order gives the sequential scan's answer.  The winner's
+// neighbour costs are read back from a per-group row buffer.
+//
+// No block-wide step: each lane reads its own 2*KT bytes of a row straight from global memory, PF rows
+// ahead of use through a register ring (the rows of a warp's columns are adjacent,
+// so a warp's loads and stores of one row are contiguous), and the only
+// synchronisation is the group's own merge of a column's lanes.  Warps therefore
+// run at their own pace instead of meeting at a barrier every row.  A lane reads back
+// only what it stored itself in the forward pass.  KT = 4 gives one column per warp
+// (the most columns in flight, for small batches); 8 and 16 trade columns for
+// disparities per lane.
+template <int KW>   // KW 32-bit words (2*KW disparities) per lane and row
+__device__ __forceinline__ void vload(const uint32_t* p, uint32_t* w) {
+  if constexpr (KW == 2) {
+    const uint2 v = __ldcg(reinterpret_cast<const uint2*>(p));
+    w[0] = v.x; w[1] = v.y;
+  } else {
+#pragma unroll
+    for (int i = 0; i < KW / 4; ++i) {
+      const uint4 v = __ldcg(reinterpret_cast<const uint4*>(p) + i);
+      w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+    }
+  }
+}
+template <int KW>
+__device__ __forceinline__ void vstore(uint32_t* p, const uint32_t* w) {
+  if constexpr (KW == 2) {
+    *reinterpret_cast<uint2*>(p) = make_uint2(w[0], w[1]);
+  } else {
+#pragma unroll
+    for (int i = 0; i < KW / 4; ++i)
+      reinterpret_cast<uint4*>(p)[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+  }
+}
+
+template <int KT, int TPCP, int PF>
+__global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b) {
+  static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
+  constexpr int KW = KT / 2;                         // 32-bit words per lane and row
   constexpr int NCOL = 256 / TPCP;                   // columns per CTA tile
-  constexpr int PFA = 8;                             // ay rows prefetched ahead
-  extern __shared__ __align__(128) uint8_t smem[];   // nstages x NCOL x maxDpad int16
   __shared__ __align__(16) int16_t sbuf[256 / 32][32 * KT];
-  __shared__ __align__(8) uint64_t bars[kMaxStages];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
   const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
-  const int tile = blockIdx.x;                        // cols_prefix counts tiles here
+  const int tile = blockIdx.x;
   const int pi = find_pair(b.cols_prefix, b.n, tile);
   const DevPair& P = b.p[pi];
   const int W = P.W, H = P.H, D = P.D, Dpad = P.Dpad;
   const int hw = cfg.hw, hh = cfg.hh, dmin = cfg.dmin;
   const int xbase = hw + dmin + (tile - b.cols_prefix[pi]) * NCOL;
-  const int ncols = min(NCOL, W - hw - xbase);        // columns with candidates
-  const int ccopy = min(NCOL, W - xbase);             // columns moved per row
-  const uint32_t row_bytes = uint32_t(ccopy) * uint32_t(Dpad) * 2u;
-  const size_t stage_bytes = size_t(NCOL) * b.maxDpad * 2;
-  const int NS = nstages;
+  const int ncols = min(NCOL, W - hw - xbase);
   const int x = xbase + gi;
   const int k0 = sub * KT;
   const bool colok = gi < ncols;
@@ -499,150 +528,143 @@ __global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b, int nstage
   const int kmax = colok ? min(D - 1, x - hw - dmin) : -1;
   const int nvalid = max(0, min(KT, kmax - k0 + 1));
   const int yin = H - hh;                             // rows >= yin have zero input
-  int* err = b.err;
-  if (tid == 0) {
-    for (int i = 0; i < NS; ++i) mbar_init(&bars[i], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  const int16_t* volt = P.vol + size_t(xbase) * Dpad;          // this tile, row 0
-  const size_t rowstride = size_t(W) * Dpad;                    // int16 per image row
-  auto issue = [&](int y, int stg) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect(&bars[stg], row_bytes);
-    bulk_load(smem + stg * stage_bytes, volt + size_t(y) * rowstride, row_bytes, &bars[stg]);
-  };
-  auto read_stage = [&](int stg, uint4* dst) {
-    const uint4* src = reinterpret_cast<const uint4*>(smem + stg * stage_bytes +
-                                                      (size_t(gi) * Dpad + k0) * 2);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) dst[v] = live ? src[v] : make_uint4(0, 0, 0, 0);
-  };
+  const size_t grs = size_t(W) * Dpad / 2;            // image-row stride in words
+  // Every lane reads a valid address (lanes without a column or past Dpad read one
+  // they never use), so the loads need no guard; only live lanes store.
+  uint32_t* gcol = reinterpret_cast<uint32_t*>(P.vol + size_t(colok ? x : xbase) * Dpad +
+                                               (live ? k0 : 0));
+  const uint16_t* ay = P.ay + (colok ? x : xbase);
   int32_t st[KT];
 #pragma unroll
   for (int s = 0; s < KT; ++s) st[s] = 0;
-  auto step = [&](const uint4* src, int32_t a) {
+  auto step = [&](const uint32_t* w, int32_t a) {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      const uint32_t w[4] = {src[v].x, src[v].y, src[v].z, src[v].w};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        st[8 * v + 2 * j] = rf_step(sx16(w[j]), st[8 * v + 2 * j], a);
-        st[8 * v + 2 * j + 1] = rf_step(hx16(w[j]), st[8 * v + 2 * j + 1], a);
-      }
+    for (int i = 0; i < KW; ++i) {
+      st[2 * i] = rf_step(sx16(w[i]), st[2 * i], a);
+      st[2 * i + 1] = rf_step(hx16(w[i]), st[2 * i + 1], a);
     }
   };
-  auto packed = [&](int v) {
-    return make_uint4(pk16(st[8 * v], st[8 * v + 1]), pk16(st[8 * v + 2], st[8 * v + 3]),
-                      pk16(st[8 * v + 4], st[8 * v + 5]), pk16(st[8 * v + 6], st[8 * v + 7]));
+  auto pack_state = [&](uint32_t* w) {
+#pragma unroll
+    for (int i = 0; i < KW; ++i) w[i] = pk16(st[2 * i], st[2 * i + 1]);
   };
-  uint4* gcol = reinterpret_cast<uint4*>(P.vol + size_t(x) * Dpad + (live ? k0 : 0));
-  const size_t grs = rowstride / 8;                   // image-row stride in uint4
-  const uint16_t* ay = P.ay + (colok ? x : xbase);
-  uint32_t phase = 0;
+  auto fetch = [&](int y, uint32_t* dst) { vload<KW>(gcol + size_t(y) * grs, dst); };
+  // The steady-state loops below run whole blocks of PF rows with no branch, so a
+  // load issued PF rows ahead stays in flight until its row; a guarded tail finishes.
+  uint32_t ring[PF][KW] = {};
+  int32_t aring[PF] = {};
+  const int ylast = clampi(yin - 1, 0, H - 1);        // last row with input
   // ---- vertical forward, rows hh..H-1, results stored in place --------------------
-  if (tid == 0)
-    for (int q = 0; q < NS && hh + q < yin; ++q) issue(hh + q, q);
-  int32_t aring[PFA];
+  auto fwd = [&](int y, int j) {
+    uint32_t c[KW];
 #pragma unroll
-  for (int j = 0; j < PFA; ++j) aring[j] = (hh + j < H) ? ay[size_t(hh + j) * W] : 0;
-  int stg = 0;
-  for (int y0 = hh; y0 < H; y0 += PFA) {
-#pragma unroll
-    for (int j = 0; j < PFA; ++j) {
-      const int y = y0 + j;
-      if (y < H) {
-        const int32_t a = aring[j];
-        aring[j] = (y + PFA < H) ? ay[size_t(y + PFA) * W] : 0;
-        uint4 c[NV];
-        if (y < yin) {
-          mbar_wait(&bars[stg], (phase >> stg) & 1u, err);
-          phase ^= 1u << stg;
-          read_stage(stg, c);
-        } else {
-#pragma unroll
-          for (int v = 0; v < NV; ++v) c[v] = make_uint4(0, 0, 0, 0);
-        }
-        step(c, a);
-        if (live) {
-#pragma unroll
-          for (int v = 0; v < NV; ++v) gcol[size_t(y) * grs + v] = packed(v);
-        }
-        if (y < yin) {
-          __syncthreads();                            // stage consumed
-          if (tid == 0 && y + NS < yin) issue(y + NS, stg);
-          stg = (stg + 1 == NS) ? 0 : stg + 1;
-        }
-      }
+    for (int i = 0; i < KW; ++i) c[i] = (y < yin) ? ring[j][i] : 0u;
+    const int32_t a = aring[j];
+    const int yn = y + PF;
+    fetch(min(yn, ylast), ring[j]);
+    aring[j] = ay[size_t(min(yn, H - 1)) * W];
+    step(c, a);
+    if (live) {
+      uint32_t o[KW];
+      pack_state(o);
+      vstore<KW>(gcol + size_t(y) * grs, o);
     }
+  };
+#pragma unroll
+  for (int j = 0; j < PF; ++j) {
+    fetch(min(hh + j, ylast), ring[j]);
+    aring[j] = ay[size_t(min(hh + j, H - 1)) * W];
   }
+  int y0 = hh;
+  for (; y0 + PF <= H; y0 += PF) {
+#pragma unroll
+    for (int j = 0; j < PF; ++j) fwd(y0 + j, j);
+  }
+#pragma unroll
+  for (int j = 0; j < PF; ++j)
+    if (y0 + j < H) fwd(y0 + j, j);
   // ---- vertical backward from H-1 (its value is the forward one) + top-2 ----------
-  fence_proxy_async();
-  __syncthreads();
-  if (tid == 0)
-    for (int q = 0; q < NS && H - 2 - q >= hh; ++q) issue(H - 2 - q, q);
-#pragma unroll
-  for (int j = 0; j < PFA; ++j) aring[j] = (H - 1 - j >= hh + 1) ? ay[size_t(H - 1 - j) * W] : 0;
-  uint32_t* rkey = P.rkey;
-  int16_t* rowbuf = &sbuf[wib][gbase * KT];
-  stg = 0;
-  for (int y0 = H - 2; y0 >= hh; y0 -= PFA) {
-#pragma unroll
-    for (int j = 0; j < PFA; ++j) {
-      const int y = y0 - j;
-      if (y >= hh) {
-        const int32_t a = aring[j];                   // coefficient at y + 1
-        aring[j] = (y + 1 - PFA >= hh + 1) ? ay[size_t(y + 1 - PFA) * W] : 0;
-        mbar_wait(&bars[stg], (phase >> stg) & 1u, err);
-        phase ^= 1u << stg;
-        uint4 c[NV];
-        read_stage(stg, c);
-        step(c, a);
-        if (y < yin) {
-          uint32_t pk0 = 0, pk1 = 0;
-#pragma unroll
-          for (int s = 0; s < KT; ++s) {
-            if (s < nvalid) {
-              const uint32_t key = (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s);
-              const uint32_t lo = min(pk0, key);
-              pk0 = max(pk0, key);
-              pk1 = max(pk1, lo);
-            }
-          }
-          if (rkey) {
-            const size_t rowo = size_t(y) * W + x - dmin - k0;
-#pragma unroll
-            for (int s = 0; s < KT; ++s)
-              if (s < nvalid)
-                atomicMax(rkey + rowo - s, (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s));
-          }
-#pragma unroll
-          for (int v = 0; v < NV; ++v) reinterpret_cast<uint4*>(rowbuf + k0)[v] = packed(v);
-#pragma unroll
-          for (int off = TPCP / 2; off > 0; off >>= 1) {
-            const uint32_t o0 = __shfl_xor_sync(gmask, pk0, off, TPCP);
-            const uint32_t o1 = __shfl_xor_sync(gmask, pk1, off, TPCP);
-            const uint32_t lo = min(pk0, o0);
-            pk0 = max(pk0, o0);
-            pk1 = max(max(pk1, o1), lo);
-          }
-          __syncwarp(gmask);
-          if (sub == 0 && colok) {
-            const int kw = pk0 ? 255 - int(pk0 & 255u) : -1;
-            const int32_t nm = (kw >= 1) ? int32_t(rowbuf[kw - 1]) : -32768;
-            const int32_t np = (kw >= 0 && kw + 1 <= kmax) ? int32_t(rowbuf[kw + 1]) : -32768;
-            const size_t i = size_t(y) * W + x;
-            P.key0[i] = pk0;
-            P.key1[i] = pk1;
-            P.nb[i] = pk16(nm, np);
-          }
-        }
-        __syncthreads();                              // stage and row buffer consumed
-        if (tid == 0 && y - NS >= hh) issue(y - NS, stg);
-        stg = (stg + 1 == NS) ? 0 : stg + 1;
-      }
-    }
+  // Rows yin..H-2 carry no candidates: plain steps with direct loads.
+  int ys = H - 2;
+  for (; ys >= yin && ys >= hh; --ys) {
+    uint32_t c[KW];
+    fetch(ys, c);
+    step(c, ay[size_t(ys + 1) * W]);
   }
+  if (ys < hh) return;
+  int16_t* rowbuf = &sbuf[wib][gbase * KT];
+  constexpr int kRowbufLast = TPCP * KT - 1;          // the group's last rowbuf entry
+  auto bwd_rows = [&](auto with_rkey) {
+    constexpr bool RK = decltype(with_rkey)::value;
+    auto bwd = [&](int y, int j) {
+      uint32_t c[KW];
+#pragma unroll
+      for (int i = 0; i < KW; ++i) c[i] = ring[j][i];
+      const int32_t a = aring[j];
+      const int yn = y - PF;
+      fetch(max(yn, 0), ring[j]);
+      aring[j] = ay[size_t(max(yn + 1, 0)) * W];
+      step(c, a);
+      uint32_t pk0 = 0, pk1 = 0;                      // key 0 never displaces a candidate
+#pragma unroll
+      for (int s = 0; s < KT; ++s) {
+        const uint32_t key =
+            (s < nvalid) ? (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s) : 0u;
+        const uint32_t lo = min(pk0, key);
+        pk0 = max(pk0, key);
+        pk1 = max(pk1, lo);
+      }
+      if (RK) {
+        const size_t rowo = size_t(y) * W + x - dmin - k0;
+#pragma unroll
+        for (int s = 0; s < KT; ++s)
+          if (s < nvalid)
+            atomicMax(P.rkey + rowo - s, (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s));
+      }
+      __syncwarp(gmask);                              // previous row's reads are done
+      {
+        uint32_t o[KW];
+        pack_state(o);
+        vstore<KW>(reinterpret_cast<uint32_t*>(rowbuf + k0), o);
+      }
+#pragma unroll
+      for (int off = TPCP / 2; off > 0; off >>= 1) {
+        const uint32_t o0 = __shfl_xor_sync(gmask, pk0, off, TPCP);
+        const uint32_t o1 = __shfl_xor_sync(gmask, pk1, off, TPCP);
+        const uint32_t lo = min(pk0, o0);
+        pk0 = max(pk0, o0);
+        pk1 = max(max(pk1, o1), lo);
+      }
+      __syncwarp(gmask);
+      // every lane of the group holds the merged keys; lane 0 writes them
+      const int kw = pk0 ? 255 - int(pk0 & 255u) : -1;
+      const int32_t vm = rowbuf[max(kw - 1, 0)];
+      const int32_t vp = rowbuf[min(kw + 1, kRowbufLast)];
+      const int32_t nm = (kw >= 1) ? vm : -32768;
+      const int32_t np = (kw >= 0 && kw + 1 <= kmax) ? vp : -32768;
+      if (sub == 0 && colok) {
+        const size_t i = size_t(y) * W + x;
+        P.key0[i] = pk0;
+        P.key1[i] = pk1;
+        P.nb[i] = pk16(nm, np);
+      }
+    };
+#pragma unroll
+    for (int j = 0; j < PF; ++j) {
+      fetch(max(ys - j, 0), ring[j]);
+      aring[j] = ay[size_t(max(ys - j + 1, 0)) * W];   // coefficient at y + 1
+    }
+    int yb = ys;
+    for (; yb - PF + 1 >= hh; yb -= PF) {
+#pragma unroll
+      for (int j = 0; j < PF; ++j) bwd(yb - j, j);
+    }
+#pragma unroll
+    for (int j = 0; j < PF; ++j)
+      if (yb - j >= hh) bwd(yb - j, j);
+  };
+  if (P.rkey) bwd_rows(std::integral_constant<bool, true>());
+  else bwd_rows(std::integral_constant<bool, false>());
 }
 
 // ---------------------------------------------------------------------------------
@@ -1002,9 +1024,9 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
 }
 
 struct de_cfg_hw { int hw, dmin; };
-int g_cols_stage_kb = 32;         // column kernel: shared bytes for the row ring
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
 int g_solve_threads = 256;        // threads per row in the solve
+int g_cols_pf = 8;                // rows the column kernel prefetches: 4 or 8
 
 template <bool PACKED, int TS, int G>
 cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
@@ -1066,7 +1088,7 @@ int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
 
 template <int KT, int TPCP>
 cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& hwc,
-                          cudaStream_t s) {
+                                 cudaStream_t s) {
   constexpr int NCOL = 256 / TPCP;
   thread_local Batch b;                               // tiles instead of columns
   b = b0;
@@ -1077,37 +1099,48 @@ cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& h
   }
   const int tiles = b.cols_prefix[b.n];
   if (tiles == 0) return cudaSuccess;
-  const size_t stage = size_t(NCOL) * b.maxDpad * 2;
-  const int ns = int(std::max<size_t>(3, std::min<size_t>(kMaxStages, g_cols_stage_kb * 1024 / stage)));
-  const size_t sm = stage * ns;
-  cudaError_t e = set_smem(k_cols<KT, TPCP>, sm);
-  if (e != cudaSuccess) return e;
-  k_cols<KT, TPCP><<<tiles, 256, sm, s>>>(cfg, b, ns);
+  // PF = 8 only where its ring still fits the register budget without spilling
+  if constexpr (KT == 4 || (KT == 8 && TPCP <= 16)) {
+    if (g_cols_pf == 8) {
+      k_cols<KT, TPCP, 8><<<tiles, 256, 0, s>>>(cfg, b);
+      return cudaGetLastError();
+    }
+  }
+  k_cols<KT, TPCP, 4><<<tiles, 256, 0, s>>>(cfg, b);
   return cudaGetLastError();
 }
 
-int g_cols_kt = 0;                // 0 = by batch size, else 8 or 16 disparities per lane
-void set_cols_kt(int v) { g_cols_kt = (v == 8 || v == 16) ? v : 0; }
-int get_cols_kt() { return g_cols_kt; }
-void set_cols_stage_kb(int v) { g_cols_stage_kb = v < 4 ? 4 : (v > 160 ? 160 : v); }
-int get_cols_stage_kb() { return g_cols_stage_kb; }
+void set_cols_pf(int v) { g_cols_pf = v == 8 ? 8 : 4; }
+int get_cols_pf() { return g_cols_pf; }
 
-// Lanes per column: Dpad/KT rounded up to a power of two; KT = 16 unless the batch is
-// small, where more, narrower lanes per column buy parallelism.
+int g_cols_kt = 0;                // 0 = by batch size, else 4, 8 or 16 disparities per lane
+void set_cols_kt(int v) { g_cols_kt = (v == 4 || v == 8 || v == 16) ? v : 0; }
+int get_cols_kt() { return g_cols_kt; }
+
+// Disparities per lane KT; lanes per column Dpad/KT rounded up to a power of two.
+// By default KT = 4 for batches too small to fill the GPU with columns (one column
+// per warp, the most columns in flight), else KT = 8.  KT = 4 needs Dpad <= 128 (32
+// lanes), KT = 16 needs Dpad >= 128.
 cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   if (b.cols_prefix[b.n] == 0) return cudaSuccess;
   const de_cfg_hw hwc{cfg.hw, cfg.dmin};
-  const int cols = b.cols_prefix[b.n];
+  const long work = long(b.cols_prefix[b.n]) * b.maxDpad;
   const int maxDpad = b.maxDpad;
-  const bool small = g_cols_kt ? g_cols_kt == 8 : long(cols) * maxDpad < 148L * 32 * 16 * 16;
-  if (small || maxDpad <= 64) {
-    switch (maxDpad) {          // KT = 8
+  int kt = g_cols_kt ? g_cols_kt : (work < 148L * 32 * 16 * 4 ? 4 : 8);
+  if (kt == 4 && maxDpad > 128) kt = 8;
+  if (kt == 16 && maxDpad <= 64) kt = 8;
+  if (kt == 4) {
+    if (maxDpad <= 64) return launch_cols_t<4, 16>(cfg, b, hwc, s);
+    return launch_cols_t<4, 32>(cfg, b, hwc, s);
+  }
+  if (kt == 8) {
+    switch (maxDpad) {
       case 64: return launch_cols_t<8, 8>(cfg, b, hwc, s);
       case 128: return launch_cols_t<8, 16>(cfg, b, hwc, s);
       default: return launch_cols_t<8, 32>(cfg, b, hwc, s);
     }
   }
-  switch (maxDpad) {            // KT = 16
+  switch (maxDpad) {
     case 128: return launch_cols_t<16, 8>(cfg, b, hwc, s);
     default: return launch_cols_t<16, 16>(cfg, b, hwc, s);
   }

@@ -80,7 +80,6 @@ int set_error(int code, const char* fmt, ...);
 void make_dev_cfg(const de_cfg& c, DevCfg* out);
 size_t pair_workspace_bytes(int W, int H, int D, bool lrc);
 void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc);
-constexpr int kMaxStages = 16;
 constexpr size_t kStatusBytes = 256;   // head of every dense workspace
 
 // Launchers (de_dense.cu).  All enqueue on `stream` and return the launch status.
@@ -94,9 +93,9 @@ int get_rows_ctas_per_sm();
 void set_cols_kt(int v);
 void set_solve_threads(int v);
 int get_solve_threads();
-void set_cols_stage_kb(int v);
-int get_cols_stage_kb();
 int get_cols_kt();
+void set_cols_pf(int v);
+int get_cols_pf();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 // The prior-masked cost stage (de_prior.cu): one pair (b.p[0]) after its census.
 size_t prior_ws_bytes(int W, int H, int D);

@@ -50,6 +50,27 @@ class DenseResult:
     cand: Optional[np.ndarray]  # f32 (6, H, W): s1, s2, d1, d2, lrc, lrc2
 
 
+def pinned_empty(shape, dtype) -> np.ndarray:
+    """An uninitialised numpy array in page-locked host memory.  The host-pointer
+    entry points move such arrays by DMA directly, with no staging copy; the array
+    keeps its allocation alive."""
+    torch = _torch()
+    dt = np.dtype(dtype)
+    n = int(np.prod(shape)) * dt.itemsize
+    t = torch.empty(max(n, 1), dtype=torch.uint8, pin_memory=True)
+    return t.numpy()[:n].view(dt).reshape(shape)
+
+
+def new_results(shapes, want_cand: bool = False, pinned: bool = True) -> list[DenseResult]:
+    """Output buffers for ``run_dense_batch(..., out=...)``: one DenseResult per
+    (H, W), page-locked unless ``pinned`` is False."""
+    alloc = pinned_empty if pinned else np.empty
+    return [DenseResult(alloc((H, W), np.float32), alloc((H, W), np.float32),
+                        alloc((H, W), np.uint8),
+                        alloc((6, H, W), np.float32) if want_cand else None)
+            for H, W in shapes]
+
+
 class _Ctx:
     """A de_ctx (host-pointer entry points) per thread and device."""
     _tls = threading.local()

@@ -161,10 +161,11 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *   "rows_ctas_per_sm"  cap on row-kernel CTAs resident per SM (default 32, i.e.
  *                       as many as fit): fewer rows in flight keep each row's
  *                       forward pass in L2 for its backward pass
- *   "cols_kt"           disparities per lane in the column kernel: 8, 16, or 0 to
- *                       choose by batch size (default 0)
- *   "cols_stage_kb"     shared memory (KB) for the column kernel's row ring; its
- *                       depth is this over one row of a tile (default 32)
+ *   "cols_kt"           disparities per lane in the column kernel: 4, 8, 16, or 0
+ *                       to choose by batch size (default 0: 4 for batches too small
+ *                       to fill the GPU with columns, else 8)
+ *   "cols_pf"           image rows the column kernel's lanes load ahead of use:
+ *                       4 or 8 (default 8; 16 disparities per lane always use 4)
  *   "solve_threads"     threads per image row in the row solve: 128, 256 or 512
  *                       (default 256) */
 DE_API int de_set_param(const char* name, int value);

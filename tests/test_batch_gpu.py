@@ -84,7 +84,7 @@ def test_graph_replay_matches_direct_launch(de, batch):
     g.close()
 
 
-@pytest.mark.parametrize("knob", ["rows_ctas_per_sm", "cols_kt", "cols_stage_kb",
+@pytest.mark.parametrize("knob", ["rows_ctas_per_sm", "cols_kt", "cols_pf",
                                   "solve_threads"])
 def test_knobs_never_change_results(de, batch, knob):
     from doubleeye_b200 import autotune
@@ -121,3 +121,32 @@ def test_autotune_picks_and_caches(de, batch, tmp_path):
         assert again.lookup(sig) is not None
     finally:
         autotune.apply(saved)
+
+
+def test_host_batch_pinned_and_pageable_agree(de, batch):
+    """The host-pointer batch moves page-locked buffers by DMA directly and stages
+    pageable ones; any mix gives the device path's results."""
+    pairs, Ls, Rs = batch
+    cfg = de.Cfg(iters=8)
+    host = [(p.left, p.right, D) for p, (_, _, D) in zip(pairs, SHAPES)]
+    shapes = [p.left.shape for p in pairs]
+    pageable = de.run_dense_batch(host, cfg, want_cand=True)
+    pinned_in = []
+    for k, (L, R, D) in enumerate(host):
+        if k % 2 == 0:                                  # every other pair page-locked
+            hl, hr = de.pinned_empty(L.shape, np.uint8), de.pinned_empty(R.shape, np.uint8)
+            hl[...] = L
+            hr[...] = R
+            pinned_in.append((hl, hr, D))
+        else:
+            pinned_in.append((L, R, D))
+    outs = de.new_results(shapes, want_cand=True, pinned=True)
+    got = de.run_dense_batch(pinned_in, cfg, want_cand=True, out=outs)
+    assert all(g is o for g, o in zip(got, outs))       # written in place
+    m = de.DenseMatcher(cfg)
+    dev = run(de, m, Ls, Rs)
+    for k in range(len(SHAPES)):
+        for key in ("disp", "margin", "conf", "cand"):
+            a, b = getattr(pageable[k], key), getattr(got[k], key)
+            assert same(torch.from_numpy(a), torch.from_numpy(b)), (k, key)
+            assert same(torch.from_numpy(np.ascontiguousarray(b)), dev[k][key]), (k, key)

@@ -99,6 +99,8 @@ SIGNATURES = {
     "de_set_param": (C.c_int, [C.c_char_p, C.c_int]),
     "de_get_param": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     "de_stage_times": (C.c_int, [C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
+    "de_int_probe": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_float),
+                              C.POINTER(C.c_double)]),
     "de_ctx_create": (C.c_int, [C.POINTER(DeCfg), C.c_int, C.POINTER(vp)]),
     "de_ctx_destroy": (C.c_int, [vp]),
     "de_ctx_set_cfg": (C.c_int, [vp, C.POINTER(DeCfg)]),

@@ -18,7 +18,7 @@ OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdoubleeye_b200.so")
 
 SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu",
-           "de_serve.cu", "de_graph.cu", "de_prior.cu"]
+           "de_serve.cu", "de_graph.cu", "de_prior.cu", "de_probe.cu"]
 TOOLS = os.path.join(PKG, "tools")
 CLI = os.path.join(OUT_DIR, "de_dense_gpu")      # the reference-compatible command line
 NVCC_FLAGS = [

@@ -156,6 +156,14 @@ DE_API int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const 
 DE_API int de_stage_timing(int enable);
 DE_API int de_stage_times(float* ms, int n, int* launches);
 
+/* Integer-pipe throughput probe (no counterpart in the reference): runs op 0 add.u32,
+ * 1 lop3.b32, 2 shf (funnel rotate), 3 mad.lo.u32 or 4 popc.b32 as 8 independent
+ * chains per thread on every SM for `trips` loop trips; *ms is the CUDA-event time
+ * of the timed launch and *lane_ops the warp-lane operations it executed, so
+ * lane_ops / (ms * SM clock * SMs) is the op's rate per SM clock.  The denominators
+ * of the dense kernels' integer roofline. */
+DE_API int de_int_probe(int op, int trips, void* stream, float* ms, double* lane_ops);
+
 /* Launch-shape knobs (process-wide; results never depend on them, only speed).
  * No counterpart in the reference, whose launch shapes are fixed.
  *   "rows_ctas_per_sm"  cap on row-kernel CTAs resident per SM (default 32, i.e.

@@ -199,3 +199,21 @@ def test_bad_arguments_raise():
     big = np.zeros((16, 16), np.uint8)
     with pytest.raises(DeError):
         de.run_dense(big, big, de.Cfg(dmax=400))     # D beyond 256
+
+
+def test_int_probe_rates():
+    """The integer-pipe probe behind the integer roofline: every op reports a rate
+    per SM clock in a physically possible range (at most 128 lanes, the two
+    integer-capable pipes), with POPC on its slower pipe."""
+    import ctypes as C
+    import torch
+    from doubleeye_b200._lib import lib
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    max_hz = 2.2e9                                     # above any B200 boost clock
+    for op in range(5):
+        ms, n = C.c_float(), C.c_double()
+        assert lib().de_int_probe(op, 200, None, C.byref(ms), C.byref(n)) == 0
+        assert ms.value > 0 and n.value > 0
+        per_clk = n.value / (ms.value * 1e-3) / sms / max_hz
+        assert 4.0 < per_clk < 160.0, (op, per_clk)
+    assert lib().de_int_probe(7, 10, None, C.byref(ms), C.byref(n)) != 0

@@ -217,3 +217,43 @@ def test_int_probe_rates():
         per_clk = n.value / (ms.value * 1e-3) / sms / max_hz
         assert 4.0 < per_clk < 160.0, (op, per_clk)
     assert lib().de_int_probe(7, 10, None, C.byref(ms), C.byref(n)) != 0
+
+
+COL_SHAPES = [
+    (40, 8, dict(dmax=16)),               # two valid rows (the smallest image)
+    (97, 9, dict(dmax=16)),               # fewer rows than the prefetch depth
+    (130, 12, dict(dmax=64)),
+    (200, 50, dict(dmin=3, dmax=130)),
+    (160, 21, dict(dmax=192)),            # 24 lanes of 8 padded to 32
+    (300, 40, dict(dmax=256)),
+    (848, 480, dict(dmax=128)),           # the benchmark shape
+]
+_COL_ORACLE = {}
+
+
+@pytest.mark.parametrize("kt,pf", [(4, 4), (4, 8), (8, 4), (8, 8), (16, 4)])
+@pytest.mark.parametrize("W,H,kw", COL_SHAPES)
+def test_column_kernel_shapes_bit_exact(oracle, W, H, kw, kt, pf):
+    """Every column-kernel shape (disparities per lane, prefetch depth) against the
+    oracle, including images shorter than the prefetch depth."""
+    from doubleeye_b200 import _lib
+    key = (W, H, tuple(sorted(kw.items())))
+    p = synth.slanted_planes(W, H, min(kw["dmax"], 3 * W // 4), tag=f"cols{W}x{H}")
+    cfg, ocfg = both(**kw)
+    if key not in _COL_ORACLE:
+        _COL_ORACLE[key] = oracle.cost_top2(ocfg, p.left, p.right)
+    ocs, ocd, ocn, ocnb = _COL_ORACLE[key]
+    saved = (_lib.get_param("cols_kt"), _lib.get_param("cols_pf"))
+    try:
+        _lib.set_param("cols_kt", kt)
+        _lib.set_param("cols_pf", pf)
+        cs, cd, cn, cnb = (t.cpu().numpy() for t in de.cost_top2(dev(p.left), dev(p.right), cfg))
+    finally:
+        _lib.set_param("cols_kt", saved[0])
+        _lib.set_param("cols_pf", saved[1])
+    assert (cn == ocn).all()
+    m = np.arange(2)[None, None, :] < cn[..., None]
+    assert (cs[m] == ocs[m]).all()
+    assert (cd[m] == ocd[m]).all()
+    win = (cn > 0)[..., None].repeat(2, -1)
+    assert (cnb[win] == ocnb[win]).all()

@@ -104,17 +104,41 @@ def ncu_traffic() -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled during the timed region:
+    every 5 ms through NVML in a thread (read-only queries), else nvidia-smi every
+    100 ms.  The NVML device is the CUDA device's, matched by PCI bus id."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+        self.samples: list[tuple[float, float, int]] = []      # (sm MHz, max MHz, reasons)
         self.lines: list[str] = []
 
+    def _nvml_handle(self):
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
+        except Exception:
+            return None
+
     def __enter__(self):
+        h = self._nvml_handle()
+        if h is not None:
+            self.nvml = h
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
@@ -126,11 +150,27 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv, h = self.nvml
+        mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), mx,
+                                     int(get_reasons(h))))
+            except Exception:
+                break
+            self.stop.wait(0.005)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nvml is not None:
+            self.t.join(timeout=2)
         if self.proc:
             self.proc.terminate()
             try:
@@ -140,7 +180,11 @@ class ClockSampler:
 
     def summary(self) -> dict:
         sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for c, m, r in self.samples:
+            sm.append(c)
+            mx.append(m)
+            reasons |= {n for n, bit in self.REASONS.items() if r & bit}
+        names = list(self.REASONS)
         for ln in self.lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 8:
@@ -155,7 +199,7 @@ class ClockSampler:
                     reasons.add(n)
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.samples else "nvidia-smi"}
 
 
 def make_pairs(n: int, seed0: int):

@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b) {
 // ---------------------------------------------------------------------------------
 // k_solve: the row solve, core/include/doubleeye/dense_solve.hpp:213-452 (K = 2,
 // candidates from the cost stage), plus the --out-conf planes and the confidence
-// (:158-171).  One CTA per row; shared-memory working set ~53 bytes per pixel.
+// (:158-171).  One CTA per row; shared-memory working set 49 bytes per pixel.
 
 
 __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }
@@ -731,24 +731,26 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   const float lambda = cfg.lambda, gamma = cfg.gamma, damping = cfg.damping, keep = cfg.keep;
   // Candidate state lives in bucket-sorted POSITION order: the members of a right
   // pixel's bucket are contiguous, candidates that claim no right pixel follow them.
-  // Shared bytes per pixel: cs 8, beta 8, rho 8, lohi 8, item 4, pos 4, margin 4,
-  // best 4, start 4, cur 4, cd 2, rev 2, cn 1, bestj 1, win 1 = 63.
+  // Shared bytes per pixel: cs 8, beta 8, rho 8, lohi 8, start 4, item 4, pos 4,
+  // cd 2, rev 2, cn 1 = 49 (five rows per SM at W = 848).  Arrays that are never
+  // live together share storage: the sort cursors live in beta until beta is
+  // cleared, pixel-order cs in rho until the sort, and the claim stage's best,
+  // bestj and win in lohi, which only the BP sweeps read.
   float* __restrict__ s_cs = reinterpret_cast<float*>(smem);          // [2W] by position
   float* __restrict__ s_beta = s_cs + 2 * W;                           // [2W] by position
   float* __restrict__ s_rho = s_beta + 2 * W;                          // [2W] by position (pixel-order cs first)
   int* __restrict__ s_lohi = reinterpret_cast<int*>(s_rho + 2 * W);    // [2W] bucket bounds lo | hi << 16, -1 none
-  float* __restrict__ s_margin = reinterpret_cast<float*>(s_lohi + 2 * W);   // [W]
-  float* __restrict__ s_best = s_margin + W;                           // [W]
-  int* s_start = reinterpret_cast<int*>(s_best + W);      // [W+1]
-  int* s_cur = s_start + W + 1;                           // [W]
-  int16_t* s_item = reinterpret_cast<int16_t*>(s_cur + W);   // [2W] position -> 2x + j
+  int* s_start = s_lohi + 2 * W;                          // [W+1]
+  int16_t* s_item = reinterpret_cast<int16_t*>(s_start + W + 1);   // [2W] position -> 2x + j
   int16_t* s_pos = s_item + 2 * W;                        // [2W] 2x + j -> position
   uint8_t* s_cd = reinterpret_cast<uint8_t*>(s_pos + 2 * W);  // [2W] k (valid for j < cn)
   int16_t* s_rev = reinterpret_cast<int16_t*>(s_cd + 2 * W);  // [W]
   int8_t* s_cn = reinterpret_cast<int8_t*>(s_rev + W);    // [W]
-  int8_t* s_bestj = s_cn + W;                             // [W]
-  uint8_t* s_win = reinterpret_cast<uint8_t*>(s_bestj + W);  // [W]
   float* s_cspx = s_rho;                                  // pixel-order cs until the sort
+  int* s_cur = reinterpret_cast<int*>(s_beta);            // [W] sort cursors until beta is cleared
+  float* s_best = reinterpret_cast<float*>(s_lohi);       // [W] after the BP sweeps
+  int8_t* s_bestj = reinterpret_cast<int8_t*>(s_lohi + W);     // [W] after the BP sweeps
+  uint8_t* s_win = reinterpret_cast<uint8_t*>(s_bestj + W);    // [W] after the BP sweeps
   __shared__ int warp_sums[kSolveThreads / 32];
   __shared__ int s_nitems, s_extra;
   const int tid = threadIdx.x;
@@ -776,10 +778,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     s_cn[x] = int8_t(n);
     const float alt = (n < 2) ? lambda : fmax_ref(c1, lambda);
     const float m = (n == 0) ? 0.f : c0 - alt;
-    s_margin[x] = m;
     if (P.margin) P.margin[row + x] = m;
     s_start[x] = 0;
-    s_win[x] = 0;
   }
   if (tid == 0) { s_start[W] = 0; s_extra = 0; }
   __syncthreads();
@@ -863,6 +863,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     float best = kNegBig;
     int bj = -1;
     const int n = s_cn[x];
+    s_win[x] = 0;
     for (int j = 0; j < n; ++j) {
       const int p = s_pos[2 * x + j];
       const float c = s_cs[p];
@@ -870,7 +871,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       const float bel = (cfg.iters > 0) ? (s_beta[p] + s_rho[p] - c) : c;
       if (bel > best) { best = bel; bj = j; }
     }
-    if (bj >= 0 && cfg.min_margin > 0.f && s_margin[x] < cfg.min_margin) bj = -1;
+    if (bj >= 0 && cfg.min_margin > 0.f) {
+      // the margin of stage 1, from the same two scores
+      const float c0 = s_cs[s_pos[2 * x]];
+      const float alt = (n < 2) ? lambda : fmax_ref(s_cs[s_pos[2 * x + 1]], lambda);
+      if (c0 - alt < cfg.min_margin) bj = -1;
+    }
     if (bj >= 0 && cfg.min_ratio > 0.f) {
       const float s2 = (n > 1) ? fmax_ref(s_cs[s_pos[2 * x + 1]], lambda) : lambda;
       const float c1 = fmax_ref(1.f - s_cs[s_pos[2 * x]], 1e-6f);
@@ -1005,7 +1011,7 @@ size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   return (s + 15) & ~size_t(15);
 }
 
-size_t solve_smem(int W) { return size_t(W) * 63 + 64; }
+size_t solve_smem(int W) { return size_t(W) * 49 + 64; }
 
 template <typename K>
 cudaError_t set_smem(K kernel, size_t bytes) {

@@ -6,6 +6,7 @@ onto the GPU, so every setting gives bit-identical results:
   rows_ctas_per_sm  resident row-kernel CTAs per SM (persistent grid size)
   cols_kt           column-kernel tile shape: disparities per lane (0 = by batch size)
   cols_pf           column-kernel prefetch depth: image rows loaded ahead of use
+  cols_cta          column-kernel threads per CTA (0 = by batch size)
   solve_threads     threads per row in the row solve (the BP schedule's width)
 
 ``tune`` times a batch under a coordinate-descent search over these values (CUDA
@@ -25,6 +26,7 @@ KNOBS = {
     "rows_ctas_per_sm": [4, 8, 32],
     "cols_kt": [0, 4, 8, 16],
     "cols_pf": [4, 8],
+    "cols_cta": [0, 128, 256],
     "solve_threads": [128, 256, 512],
 }
 CACHE = os.path.join(_lib.PKG, "_lib", "autotune.json")

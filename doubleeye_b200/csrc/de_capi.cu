@@ -503,6 +503,7 @@ int de_set_param(const char* name, int value) {
   if (!std::strcmp(name, "rows_ctas_per_sm")) { de::set_rows_ctas_per_sm(value); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { de::set_cols_kt(value); return DE_OK; }
   if (!std::strcmp(name, "cols_pf")) { de::set_cols_pf(value); return DE_OK; }
+  if (!std::strcmp(name, "cols_cta")) { de::set_cols_cta(value); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { de::set_solve_threads(value); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
@@ -512,6 +513,7 @@ int de_get_param(const char* name, int* value) {
   if (!std::strcmp(name, "rows_ctas_per_sm")) { *value = de::get_rows_ctas_per_sm(); return DE_OK; }
   if (!std::strcmp(name, "cols_kt")) { *value = de::get_cols_kt(); return DE_OK; }
   if (!std::strcmp(name, "cols_pf")) { *value = de::get_cols_pf(); return DE_OK; }
+  if (!std::strcmp(name, "cols_cta")) { *value = de::get_cols_cta(); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { *value = de::get_solve_threads(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }

@@ -505,12 +505,12 @@ __device__ __forceinline__ void vstore(uint32_t* p, const uint32_t* w) {
   }
 }
 
-template <int KT, int TPCP, int PF>
-__global__ void __launch_bounds__(256, 2) k_cols(DevCfg cfg, Batch b) {
+template <int KT, int TPCP, int PF, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
   constexpr int KW = KT / 2;                         // 32-bit words per lane and row
-  constexpr int NCOL = 256 / TPCP;                   // columns per CTA tile
-  __shared__ __align__(16) int16_t sbuf[256 / 32][32 * KT];
+  constexpr int NCOL = NT / TPCP;                    // columns per CTA tile
+  __shared__ __align__(16) int16_t sbuf[NT / 32][32 * KT];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
   const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
@@ -1092,10 +1092,10 @@ int get_solve_threads() { return g_solve_threads; }
 void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }
 int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
 
-template <int KT, int TPCP>
-cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& hwc,
-                                 cudaStream_t s) {
-  constexpr int NCOL = 256 / TPCP;
+template <int KT, int TPCP, int NT>
+cudaError_t launch_cols_nt(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& hwc,
+                           cudaStream_t s) {
+  constexpr int NCOL = NT / TPCP;
   thread_local Batch b;                               // tiles instead of columns
   b = b0;
   b.cols_prefix[0] = 0;
@@ -1108,12 +1108,26 @@ cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& h
   // PF = 8 only where its ring still fits the register budget without spilling
   if constexpr (KT == 4 || (KT == 8 && TPCP <= 16)) {
     if (g_cols_pf == 8) {
-      k_cols<KT, TPCP, 8><<<tiles, 256, 0, s>>>(cfg, b);
+      k_cols<KT, TPCP, 8, NT><<<tiles, NT, 0, s>>>(cfg, b);
       return cudaGetLastError();
     }
   }
-  k_cols<KT, TPCP, 4><<<tiles, 256, 0, s>>>(cfg, b);
+  k_cols<KT, TPCP, 4, NT><<<tiles, NT, 0, s>>>(cfg, b);
   return cudaGetLastError();
+}
+
+int g_cols_cta = 0;               // column-kernel CTA threads: 128, 256, or 0 = by shape
+void set_cols_cta(int v) { g_cols_cta = (v == 128 || v == 256) ? v : 0; }
+int get_cols_cta() { return g_cols_cta; }
+
+// CTA size: 128 threads while the batch is too small to give every SM several
+// 256-thread tiles (finer tiles spread the column groups over more SMs), else 256.
+template <int KT, int TPCP>
+cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b, const de_cfg_hw& hwc,
+                          cudaStream_t s, long work) {
+  const int nt = g_cols_cta ? g_cols_cta : (work < 148L * 32 * 16 * 8 ? 128 : 256);
+  if (nt == 128) return launch_cols_nt<KT, TPCP, 128>(cfg, b, hwc, s);
+  return launch_cols_nt<KT, TPCP, 256>(cfg, b, hwc, s);
 }
 
 void set_cols_pf(int v) { g_cols_pf = v == 8 ? 8 : 4; }
@@ -1136,19 +1150,19 @@ cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   if (kt == 4 && maxDpad > 128) kt = 8;
   if (kt == 16 && maxDpad <= 64) kt = 8;
   if (kt == 4) {
-    if (maxDpad <= 64) return launch_cols_t<4, 16>(cfg, b, hwc, s);
-    return launch_cols_t<4, 32>(cfg, b, hwc, s);
+    if (maxDpad <= 64) return launch_cols_t<4, 16>(cfg, b, hwc, s, work);
+    return launch_cols_t<4, 32>(cfg, b, hwc, s, work);
   }
   if (kt == 8) {
     switch (maxDpad) {
-      case 64: return launch_cols_t<8, 8>(cfg, b, hwc, s);
-      case 128: return launch_cols_t<8, 16>(cfg, b, hwc, s);
-      default: return launch_cols_t<8, 32>(cfg, b, hwc, s);
+      case 64: return launch_cols_t<8, 8>(cfg, b, hwc, s, work);
+      case 128: return launch_cols_t<8, 16>(cfg, b, hwc, s, work);
+      default: return launch_cols_t<8, 32>(cfg, b, hwc, s, work);
     }
   }
   switch (maxDpad) {
-    case 128: return launch_cols_t<16, 8>(cfg, b, hwc, s);
-    default: return launch_cols_t<16, 16>(cfg, b, hwc, s);
+    case 128: return launch_cols_t<16, 8>(cfg, b, hwc, s, work);
+    default: return launch_cols_t<16, 16>(cfg, b, hwc, s, work);
   }
 }
 

@@ -96,6 +96,8 @@ int get_solve_threads();
 int get_cols_kt();
 void set_cols_pf(int v);
 int get_cols_pf();
+void set_cols_cta(int v);
+int get_cols_cta();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 // The prior-masked cost stage (de_prior.cu): one pair (b.p[0]) after its census.
 size_t prior_ws_bytes(int W, int H, int D);

@@ -231,11 +231,12 @@ COL_SHAPES = [
 _COL_ORACLE = {}
 
 
+@pytest.mark.parametrize("cta", [128, 256])
 @pytest.mark.parametrize("kt,pf", [(4, 4), (4, 8), (8, 4), (8, 8), (16, 4)])
 @pytest.mark.parametrize("W,H,kw", COL_SHAPES)
-def test_column_kernel_shapes_bit_exact(oracle, W, H, kw, kt, pf):
-    """Every column-kernel shape (disparities per lane, prefetch depth) against the
-    oracle, including images shorter than the prefetch depth."""
+def test_column_kernel_shapes_bit_exact(oracle, W, H, kw, kt, pf, cta):
+    """Every column-kernel shape (disparities per lane, prefetch depth, CTA size)
+    against the oracle, including images shorter than the prefetch depth."""
     from doubleeye_b200 import _lib
     key = (W, H, tuple(sorted(kw.items())))
     p = synth.slanted_planes(W, H, min(kw["dmax"], 3 * W // 4), tag=f"cols{W}x{H}")
@@ -243,14 +244,15 @@ def test_column_kernel_shapes_bit_exact(oracle, W, H, kw, kt, pf):
     if key not in _COL_ORACLE:
         _COL_ORACLE[key] = oracle.cost_top2(ocfg, p.left, p.right)
     ocs, ocd, ocn, ocnb = _COL_ORACLE[key]
-    saved = (_lib.get_param("cols_kt"), _lib.get_param("cols_pf"))
+    names = ("cols_kt", "cols_pf", "cols_cta")
+    saved = [_lib.get_param(n) for n in names]
     try:
-        _lib.set_param("cols_kt", kt)
-        _lib.set_param("cols_pf", pf)
+        for n, v in zip(names, (kt, pf, cta)):
+            _lib.set_param(n, v)
         cs, cd, cn, cnb = (t.cpu().numpy() for t in de.cost_top2(dev(p.left), dev(p.right), cfg))
     finally:
-        _lib.set_param("cols_kt", saved[0])
-        _lib.set_param("cols_pf", saved[1])
+        for n, v in zip(names, saved):
+            _lib.set_param(n, v)
     assert (cn == ocn).all()
     m = np.arange(2)[None, None, :] < cn[..., None]
     assert (cs[m] == ocs[m]).all()

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <algorithm>
 #include <mutex>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -629,13 +630,24 @@ void parallel_copy(const std::vector<HostCopy>& jobs) {
     for (size_t o = 0; o < j.n; o += piece)
       pieces.push_back({static_cast<uint8_t*>(j.dst) + o, static_cast<const uint8_t*>(j.src) + o,
                         std::min(piece, j.n - o)});
+  // Worker t copies pieces t, t + nt, ...; the calling thread does the share of any
+  // worker it could not start (no exception leaves this C-ABI path).
   std::vector<std::thread> th;
-  for (int t = 1; t < nt; ++t)
-    th.emplace_back([&pieces, t, nt] {
-      for (size_t k = t; k < pieces.size(); k += nt)
-        std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
-    });
-  for (size_t k = 0; k < pieces.size(); k += nt) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
+  th.reserve(nt - 1);
+  auto share = [&pieces, nt](int t) {
+    for (size_t k = t; k < pieces.size(); k += nt)
+      std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
+  };
+  int started = 1;
+  for (int t = 1; t < nt; ++t, ++started) {
+    try {
+      th.emplace_back(share, t);
+    } catch (const std::system_error&) {
+      break;
+    }
+  }
+  share(0);
+  for (int t = started; t < nt; ++t) share(t);
   for (std::thread& t : th) t.join();
 }
 

@@ -758,8 +758,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   const size_t row = size_t(y) * W;
   const float q = 1.f / 16384.f;
 
-  // 1. candidates + margin (dense_solve.hpp:263-268)
-  for (int x = tid; x < W; x += kSolveThreads) {
+  // 1. candidates + margin (dense_solve.hpp:263-268).  The packed keys of a thread's
+  //    pixels are fetched four pixels at a time before any is used, so their global
+  //    loads overlap instead of waiting one after another.
+  auto candidates = [&](int x, uint32_t a, uint32_t bb) {
     int n = 0;
     float c0 = kNegBig, c1 = kNegBig;
     int k0 = 0, k1 = 0;
@@ -767,8 +769,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       n = P.ref_cn[row + x];
       if (n > 0) { c0 = P.ref_cs[2 * (row + x)]; k0 = P.ref_cd[2 * (row + x)]; }
       if (n > 1) { c1 = P.ref_cs[2 * (row + x) + 1]; k1 = P.ref_cd[2 * (row + x) + 1]; }
-    } else if (row_ok && x >= hw + dmin && x < W - hw) {
-      const uint32_t a = P.key0[row + x], bb = P.key1[row + x];
+    } else {
       if (a) { c0 = float(int32_t(a >> 8) - 32768) * q; k0 = 255 - int(a & 255u); n = 1; }
       if (bb) { c1 = float(int32_t(bb >> 8) - 32768) * q; k1 = 255 - int(bb & 255u); n = 2; }
     }
@@ -780,6 +781,19 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     const float m = (n == 0) ? 0.f : c0 - alt;
     if (P.margin) P.margin[row + x] = m;
     s_start[x] = 0;
+  };
+  for (int xb = tid; xb < W; xb += 4 * kSolveThreads) {
+    uint32_t a[4], bb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int x = xb + u * kSolveThreads;
+      const bool ok = !REF_LAYOUT && row_ok && x >= hw + dmin && x < W - hw;
+      a[u] = ok ? P.key0[row + x] : 0u;
+      bb[u] = ok ? P.key1[row + x] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (xb + u * kSolveThreads < W) candidates(xb + u * kSolveThreads, a[u], bb[u]);
   }
   if (tid == 0) { s_start[W] = 0; s_extra = 0; }
   __syncthreads();
@@ -905,7 +919,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   // 7. outputs: disparity with sub-pixel fit (:380-434), reverse-match residuals
   //    (:442-451, core/tools/de_dense.cpp:1581-1597), candidate planes, confidence
   const size_t WH = size_t(W) * H;
-  for (int x = tid; x < W; x += kSolveThreads) {
+  auto outputs = [&](int x, uint32_t nb) {
     float dl = __int_as_float(0x7fc00000);
     const int n = s_cn[x];
     const float2 cs2 = make_float2(n > 0 ? s_cs[s_pos[2 * x]] : kNegBig,
@@ -919,7 +933,6 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
         if (REF_LAYOUT) {
           if (P.ref_cnb) { m16 = P.ref_cnb[2 * (row + x)]; p16 = P.ref_cnb[2 * (row + x) + 1]; }
         } else {
-          const uint32_t nb = P.nb[row + x];
           m16 = lo16(nb); p16 = hi16(nb);
         }
         const float c0 = cs2.x;
@@ -968,6 +981,19 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
         cv = uint8_t(lroundf(confidence_dev(s1, s2, lambda, (lrc2 == lrc2) ? lrc2 : 0.f, 1.f) * 255.f));
       P.conf[row + x] = cv;
     }
+  };
+  // the neighbour words of a thread's pixels, four at a time, loads first
+  const bool want_nb = !REF_LAYOUT && cfg.subpixel;
+  for (int xb = tid; xb < W; xb += 4 * kSolveThreads) {
+    uint32_t nb[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int x = xb + u * kSolveThreads;
+      nb[u] = (want_nb && x < W && s_win[x]) ? P.nb[row + x] : 0x80008000u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (xb + u * kSolveThreads < W) outputs(xb + u * kSolveThreads, nb[u]);
   }
 }
 

@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
   constexpr int KW = KT / 2;                         // 32-bit words per lane and row
   constexpr int NCOL = NT / TPCP;                    // columns per CTA tile
-  __shared__ __align__(16) int16_t sbuf[NT / 32][32 * KT];
+  __shared__ __align__(16) int16_t sbuf[NT / 32][2][32 * KT];   // two row buffers per warp
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
   const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
@@ -592,11 +592,13 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
     step(c, ay[size_t(ys + 1) * W]);
   }
   if (ys < hh) return;
-  int16_t* rowbuf = &sbuf[wib][gbase * KT];
+  int16_t* rowbufs[2] = {&sbuf[wib][0][gbase * KT], &sbuf[wib][1][gbase * KT]};
   constexpr int kRowbufLast = TPCP * KT - 1;          // the group's last rowbuf entry
   auto bwd_rows = [&](auto with_rkey) {
     constexpr bool RK = decltype(with_rkey)::value;
-    auto bwd = [&](int y, int j) {
+    // One row: the filter step, the lane's top-2 keys, and its costs into a row
+    // buffer (for the winner's neighbours).
+    auto row_keys = [&](int y, int j, uint32_t& pk0, uint32_t& pk1, int16_t* rowbuf) {
       uint32_t c[KW];
 #pragma unroll
       for (int i = 0; i < KW; ++i) c[i] = ring[j][i];
@@ -605,7 +607,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
       fetch(max(yn, 0), ring[j]);
       aring[j] = ay[size_t(max(yn + 1, 0)) * W];
       step(c, a);
-      uint32_t pk0 = 0, pk1 = 0;                      // key 0 never displaces a candidate
+      pk0 = 0;
+      pk1 = 0;                                        // key 0 never displaces a candidate
 #pragma unroll
       for (int s = 0; s < KT; ++s) {
         const uint32_t key =
@@ -621,22 +624,19 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
           if (s < nvalid)
             atomicMax(P.rkey + rowo - s, (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s));
       }
-      __syncwarp(gmask);                              // previous row's reads are done
-      {
-        uint32_t o[KW];
-        pack_state(o);
-        vstore<KW>(reinterpret_cast<uint32_t*>(rowbuf + k0), o);
-      }
-#pragma unroll
-      for (int off = TPCP / 2; off > 0; off >>= 1) {
-        const uint32_t o0 = __shfl_xor_sync(gmask, pk0, off, TPCP);
-        const uint32_t o1 = __shfl_xor_sync(gmask, pk1, off, TPCP);
-        const uint32_t lo = min(pk0, o0);
-        pk0 = max(pk0, o0);
-        pk1 = max(max(pk1, o1), lo);
-      }
-      __syncwarp(gmask);
-      // every lane of the group holds the merged keys; lane 0 writes them
+      uint32_t o[KW];
+      pack_state(o);
+      vstore<KW>(reinterpret_cast<uint32_t*>(rowbuf + k0), o);
+    };
+    auto merge_step = [&](uint32_t& pk0, uint32_t& pk1, int off) {
+      const uint32_t o0 = __shfl_xor_sync(gmask, pk0, off, TPCP);
+      const uint32_t o1 = __shfl_xor_sync(gmask, pk1, off, TPCP);
+      const uint32_t lo = min(pk0, o0);
+      pk0 = max(pk0, o0);
+      pk1 = max(max(pk1, o1), lo);
+    };
+    // every lane of the group holds the merged keys; lane 0 writes them
+    auto emit = [&](int y, uint32_t pk0, uint32_t pk1, const int16_t* rowbuf) {
       const int kw = pk0 ? 255 - int(pk0 & 255u) : -1;
       const int32_t vm = rowbuf[max(kw - 1, 0)];
       const int32_t vp = rowbuf[min(kw + 1, kRowbufLast)];
@@ -649,15 +649,41 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
         P.nb[i] = pk16(nm, np);
       }
     };
+    auto bwd = [&](int y, int j) {                   // one row
+      uint32_t pk0, pk1;
+      __syncwarp(gmask);                              // the previous rows' reads are done
+      row_keys(y, j, pk0, pk1, rowbufs[0]);
+#pragma unroll
+      for (int off = TPCP / 2; off > 0; off >>= 1) merge_step(pk0, pk1, off);
+      __syncwarp(gmask);
+      emit(y, pk0, pk1, rowbufs[0]);
+    };
+    // Two rows at a time: their lane merges are independent (only the filter state
+    // runs from row to row), so the two shuffle chains interleave.
+    auto bwd2 = [&](int y, int j) {                   // rows y and y - 1
+      uint32_t a0, a1, b0, b1;
+      __syncwarp(gmask);
+      row_keys(y, j, a0, a1, rowbufs[0]);
+      row_keys(y - 1, j + 1, b0, b1, rowbufs[1]);
+#pragma unroll
+      for (int off = TPCP / 2; off > 0; off >>= 1) {
+        merge_step(a0, a1, off);
+        merge_step(b0, b1, off);
+      }
+      __syncwarp(gmask);
+      emit(y, a0, a1, rowbufs[0]);
+      emit(y - 1, b0, b1, rowbufs[1]);
+    };
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
       fetch(max(ys - j, 0), ring[j]);
       aring[j] = ay[size_t(max(ys - j + 1, 0)) * W];   // coefficient at y + 1
     }
     int yb = ys;
+    static_assert(PF % 2 == 0, "rows are taken in pairs");
     for (; yb - PF + 1 >= hh; yb -= PF) {
 #pragma unroll
-      for (int j = 0; j < PF; ++j) bwd(yb - j, j);
+      for (int j = 0; j < PF; j += 2) bwd2(yb - j, j);
     }
 #pragma unroll
     for (int j = 0; j < PF; ++j)

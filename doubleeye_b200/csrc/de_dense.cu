@@ -510,7 +510,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
   constexpr int KW = KT / 2;                         // 32-bit words per lane and row
   constexpr int NCOL = NT / TPCP;                    // columns per CTA tile
-  __shared__ __align__(16) int16_t sbuf[NT / 32][2][32 * KT];   // two row buffers per warp
+  constexpr int kRB = KT >= 16 ? 2 : 4;              // backward rows merged together
+  __shared__ __align__(16) int16_t sbuf[NT / 32][kRB][32 * KT];   // kRB row buffers per warp
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
   const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
@@ -592,7 +593,9 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
     step(c, ay[size_t(ys + 1) * W]);
   }
   if (ys < hh) return;
-  int16_t* rowbufs[2] = {&sbuf[wib][0][gbase * KT], &sbuf[wib][1][gbase * KT]};
+  int16_t* rowbufs[kRB];
+#pragma unroll
+  for (int i = 0; i < kRB; ++i) rowbufs[i] = &sbuf[wib][i][gbase * KT];
   constexpr int kRowbufLast = TPCP * KT - 1;          // the group's last rowbuf entry
   auto bwd_rows = [&](auto with_rkey) {
     constexpr bool RK = decltype(with_rkey)::value;
@@ -658,21 +661,20 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
       __syncwarp(gmask);
       emit(y, pk0, pk1, rowbufs[0]);
     };
-    // Two rows at a time: their lane merges are independent (only the filter state
-    // runs from row to row), so the two shuffle chains interleave.
-    auto bwd2 = [&](int y, int j) {                   // rows y and y - 1
-      uint32_t a0, a1, b0, b1;
+    // kRB rows at a time: their lane merges are independent (only the filter state
+    // runs from row to row), so the shuffle chains interleave.
+    auto bwdn = [&](int y, int j) {                   // rows y, y - 1, ..., y - kRB + 1
+      uint32_t k0s[kRB], k1s[kRB];
       __syncwarp(gmask);
-      row_keys(y, j, a0, a1, rowbufs[0]);
-      row_keys(y - 1, j + 1, b0, b1, rowbufs[1]);
 #pragma unroll
-      for (int off = TPCP / 2; off > 0; off >>= 1) {
-        merge_step(a0, a1, off);
-        merge_step(b0, b1, off);
-      }
+      for (int r = 0; r < kRB; ++r) row_keys(y - r, j + r, k0s[r], k1s[r], rowbufs[r]);
+#pragma unroll
+      for (int off = TPCP / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int r = 0; r < kRB; ++r) merge_step(k0s[r], k1s[r], off);
       __syncwarp(gmask);
-      emit(y, a0, a1, rowbufs[0]);
-      emit(y - 1, b0, b1, rowbufs[1]);
+#pragma unroll
+      for (int r = 0; r < kRB; ++r) emit(y - r, k0s[r], k1s[r], rowbufs[r]);
     };
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
@@ -680,10 +682,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
       aring[j] = ay[size_t(max(ys - j + 1, 0)) * W];   // coefficient at y + 1
     }
     int yb = ys;
-    static_assert(PF % 2 == 0, "rows are taken in pairs");
+    static_assert(PF % kRB == 0, "rows are taken kRB at a time");
     for (; yb - PF + 1 >= hh; yb -= PF) {
 #pragma unroll
-      for (int j = 0; j < PF; j += 2) bwd2(yb - j, j);
+      for (int j = 0; j < PF; j += kRB) bwdn(yb - j, j);
     }
 #pragma unroll
     for (int j = 0; j < PF; ++j)

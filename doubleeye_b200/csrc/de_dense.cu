@@ -510,7 +510,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
   constexpr int KW = KT / 2;                         // 32-bit words per lane and row
   constexpr int NCOL = NT / TPCP;                    // columns per CTA tile
-  constexpr int kRB = KT >= 16 ? 2 : 4;              // backward rows merged together
+  // backward rows whose lane merges run together: the whole prefetch ring (8 rows)
+  // where it is 8 deep (at 8 disparities per lane this spills a few bytes of
+  // loop-invariant state and is still the fastest), 2 at 16 disparities per lane
+  constexpr int kRB = KT >= 16 ? 2 : (PF >= 8 ? 8 : 4);
   __shared__ __align__(16) int16_t sbuf[NT / 32][kRB][32 * KT];   // kRB row buffers per warp
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;

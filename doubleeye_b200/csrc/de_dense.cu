@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
       const uint64_t* lp = sLx + x;
       const uint16_t* ap = sax + x;
       uint32_t* op = out + x * XS;
-#pragma unroll 2
+#pragma unroll 8
       for (; x + 1 < xend; x += 2) {                  // two x per iteration
         const uint32_t a2 = *reinterpret_cast<const uint32_t*>(ap);
         const ulonglong2 l2 = *reinterpret_cast<const ulonglong2*>(lp);

@@ -895,9 +895,19 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     __syncthreads();
     for (int p = tid; p < nitems; p += kSolveThreads) {
       const int lohi = s_lohi[p];
-      const int lo = lohi & 0xFFFF, hi = lohi >> 16;
-      float ex = kNegBig;
-      for (int r = lo; r < hi; ++r)
+      const int lo = lohi & 0xFFFF, hi = lohi >> 16;     // p's bucket, hi > lo
+      // The first four members are read at once and reduced as a tree; fmax_ref
+      // keeps its left operand on ties, so the tree returns the scan's first
+      // maximum, and members past the fourth continue the scan from it.
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = lo + u;
+        const float t = s_rho[min(r, hi - 1)];
+        v[u] = (r < hi && r != p) ? t : kNegBig;
+      }
+      float ex = fmax_ref(fmax_ref(v[0], v[1]), fmax_ref(v[2], v[3]));
+      for (int r = lo + 4; r < hi; ++r)
         if (r != p) ex = fmax_ref(ex, s_rho[r]);
       s_beta[p] = keep * (s_cs[p] - fmax_ref(gamma, ex)) + damping * s_beta[p];
     }

@@ -25,7 +25,7 @@ from . import _lib
 KNOBS = {
     "rows_ctas_per_sm": [4, 8, 32],
     "cols_kt": [0, 4, 8, 16],
-    "cols_pf": [4, 8],
+    "cols_pf": [0, 4, 8, 16],
     "cols_cta": [0, 128, 256],
     "solve_threads": [128, 256, 512],
 }

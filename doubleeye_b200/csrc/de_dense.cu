@@ -513,7 +513,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   // backward rows whose lane merges run together: the whole prefetch ring (8 rows)
   // where it is 8 deep (at 8 disparities per lane this spills a few bytes of
   // loop-invariant state and is still the fastest), 2 at 16 disparities per lane
-  constexpr int kRB = KT >= 16 ? 2 : (PF >= 8 ? 8 : 4);
+  constexpr int kRB = KT >= 16 ? 2 : (PF >= 8 ? 8 : 4);   // (PF = 16 keeps 8)
   __shared__ __align__(16) int16_t sbuf[NT / 32][kRB][32 * KT];   // kRB row buffers per warp
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
@@ -862,15 +862,26 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   const int nall = nitems + s_extra;
   for (int p = tid; p < nall; p += kSolveThreads) { s_beta[p] = 0.f; s_rho[p] = 0.f; }
   // 3. reverse match over the surviving candidates (:303-313): first maximum in x order
+  //    (value desc, index asc) is a total order, so members may be folded four at a
+  //    time with their loads issued together
   for (int xr = tid; xr < W; xr += kSolveThreads) {
-    int bd = -1, bi = 1 << 30;
+    int bi = 1 << 30;
     float bv = kNegBig;
-    for (int p = s_start[xr]; p < s_start[xr + 1]; ++p) {
-      const int idx = s_item[p];
-      const float v = s_cs[p];
-      if (v > bv || (v == bv && idx < bi)) { bv = v; bd = s_cd[idx]; bi = idx; }
+    const int lo = s_start[xr], hi = s_start[xr + 1];
+    for (int p0 = lo; p0 < hi; p0 += 4) {
+      int idx[4];
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int p = min(p0 + u, hi - 1);
+        idx[u] = s_item[p];
+        v[u] = s_cs[p];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (p0 + u < hi && (v[u] > bv || (v[u] == bv && idx[u] < bi))) { bv = v[u]; bi = idx[u]; }
     }
-    s_rev[xr] = int16_t(bd);
+    s_rev[xr] = int16_t(bi < (1 << 30) ? int(s_cd[bi]) : -1);
   }
   // 4. damped max-sum iterations (:318-341): rho per pixel (its partner's beta through
   //    the position table), beta per bucket position ("max over my bucket excluding me"
@@ -944,15 +955,26 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   // 6. one-to-one claim (:359-378): each eligible pixel claims exactly one right
   //    pixel, so the sequential greedy pass equals, per right pixel, the claimant
   //    first in (belief desc, x asc) order.
+  //    (belief desc, x asc) is a total order (a bucket holds at most one candidate
+  //    per pixel), so members are folded four at a time, loads first.
   for (int xr = tid; xr < W; xr += kSolveThreads) {
     int wx = -1;
     float wb = 0.f;
-    for (int p = s_start[xr]; p < s_start[xr + 1]; ++p) {
-      const int idx = s_item[p];
-      const int x = idx >> 1, j = idx & 1;
-      if (s_bestj[x] != j) continue;
-      const float bv = s_best[x];
-      if (wx < 0 || bv > wb || (bv == wb && x < wx)) { wx = x; wb = bv; }
+    const int lo = s_start[xr], hi = s_start[xr + 1];
+    for (int p0 = lo; p0 < hi; p0 += 4) {
+      int xs[4];
+      bool el[4];
+      float bvs[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int idx = s_item[min(p0 + u, hi - 1)];
+        xs[u] = idx >> 1;
+        el[u] = p0 + u < hi && s_bestj[xs[u]] == (idx & 1);
+        bvs[u] = s_best[xs[u]];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (el[u] && (wx < 0 || bvs[u] > wb || (bvs[u] == wb && xs[u] < wx))) { wx = xs[u]; wb = bvs[u]; }
     }
     if (wx >= 0) s_win[wx] = 1;
   }
@@ -1099,7 +1121,7 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
 struct de_cfg_hw { int hw, dmin; };
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
 int g_solve_threads = 256;        // threads per row in the solve
-int g_cols_pf = 8;                // rows the column kernel prefetches: 4 or 8
+int g_cols_pf = 0;                // rows the column kernel prefetches: 4, 8, 16, 0 = by shape
 
 template <bool PACKED, int TS, int G>
 cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
@@ -1172,9 +1194,17 @@ cudaError_t launch_cols_nt(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& 
   }
   const int tiles = b.cols_prefix[b.n];
   if (tiles == 0) return cudaSuccess;
-  // PF = 8 only where its ring still fits the register budget without spilling
+  // PF = 16 at 4 disparities per lane; 8 where the ring still fits the register
+  // budget; else 4
+  const int pf = g_cols_pf ? g_cols_pf : (KT == 4 ? 16 : 8);
+  if constexpr (KT == 4) {
+    if (pf == 16) {
+      k_cols<KT, TPCP, 16, NT><<<tiles, NT, 0, s>>>(cfg, b);
+      return cudaGetLastError();
+    }
+  }
   if constexpr (KT == 4 || (KT == 8 && TPCP <= 16)) {
-    if (g_cols_pf == 8) {
+    if (pf >= 8) {
       k_cols<KT, TPCP, 8, NT><<<tiles, NT, 0, s>>>(cfg, b);
       return cudaGetLastError();
     }
@@ -1197,7 +1227,7 @@ cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b, const de_cfg_hw& hw
   return launch_cols_nt<KT, TPCP, 256>(cfg, b, hwc, s);
 }
 
-void set_cols_pf(int v) { g_cols_pf = v == 8 ? 8 : 4; }
+void set_cols_pf(int v) { g_cols_pf = (v == 4 || v == 8 || v == 16) ? v : 0; }
 int get_cols_pf() { return g_cols_pf; }
 
 int g_cols_kt = 0;                // 0 = by batch size, else 4, 8 or 16 disparities per lane

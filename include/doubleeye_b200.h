@@ -173,7 +173,9 @@ DE_API int de_int_probe(int op, int trips, void* stream, float* ms, double* lane
  *                       to choose by batch size (default 0: 4 for batches too small
  *                       to fill the GPU with columns, else 8)
  *   "cols_pf"           image rows the column kernel's lanes load ahead of use:
- *                       4 or 8 (default 8; 16 disparities per lane always use 4)
+ *                       4, 8, 16 (4 disparities per lane only), or 0 to choose by
+ *                       shape (default 0: 16 at 4 disparities per lane, else 8; 16
+ *                       disparities per lane always use 4)
  *   "cols_cta"          column-kernel threads per CTA: 128, 256, or 0 to choose by
  *                       batch size (default 0: 128 for batches of a few 848x480
  *                       pairs or less, else 256)

@@ -232,7 +232,7 @@ _COL_ORACLE = {}
 
 
 @pytest.mark.parametrize("cta", [128, 256])
-@pytest.mark.parametrize("kt,pf", [(4, 4), (4, 8), (8, 4), (8, 8), (16, 4)])
+@pytest.mark.parametrize("kt,pf", [(4, 4), (4, 8), (4, 16), (8, 4), (8, 8), (16, 4)])
 @pytest.mark.parametrize("W,H,kw", COL_SHAPES)
 def test_column_kernel_shapes_bit_exact(oracle, W, H, kw, kt, pf, cta):
     """Every column-kernel shape (disparities per lane, prefetch depth, CTA size)

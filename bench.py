@@ -397,6 +397,49 @@ def run_c5(de, local: int) -> dict:
     return out
 
 
+def run_c1(de, local: int, steps: int, warmup: int) -> dict:
+    """The sparse configuration: an 848x480 value-noise scene over fronto-parallel
+    planes at 8/24/52 px, 9x7 census.  Keypoint path on the device (FAST detection in
+    both images with 24-px cells, about 2100 keypoints each; census descriptors;
+    keypoint MASDA, 10 BP iterations), timed as one device-resident pair with CUDA
+    events; and the dense cost / filter / top-2 of the same pair at D=64 (no BP)."""
+    import torch
+    from doubleeye_b200 import sparse, synth
+    p = synth.fronto_planes()
+    dev = torch.device("cuda", local)
+    L = torch.from_numpy(p.left).to(dev)
+    R = torch.from_numpy(p.right).to(dev)
+    sm = sparse.SparseMatcher(det=sparse.DetCfg(cell=24),
+                              cfg=sparse.MatchCfg(iterations=10, census_bits=62),
+                              census=(4, 3), device=local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, n):
+        for _ in range(warmup):
+            r = fn()
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(n):
+            r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n, r
+
+    pair_ms, res = timed(lambda: sm.match_pair(L, R), steps)
+    det_ms, _ = timed(lambda: sm.detect(L), steps)
+    out = {"workload": "848x480 fronto planes 8/24/52, 9x7 census, ~2100 keypoints, "
+                       "keypoint MASDA 10 iterations",
+           "sparse_pair_ms": pair_ms, "detect_ms_per_image": det_ms,
+           "keypoints_left": int(res["nl"].item()), "keypoints_right": int(res["nr"].item()),
+           "matches": int(res["n"].item())}
+    m = de.DenseMatcher(de.Cfg(dmax=64, census_hw=4, census_hh=3), device=local)
+    for B in (1, 16):
+        items = [(L, R, 0, m.new_outputs(480, 848)) for _ in range(B)]
+        ms, _ = timed(lambda: m.match_into(items), steps)
+        out[f"dense_top2_pairs_per_s_b{B}"] = B / (ms / 1e3)
+    return out
+
+
 def run_c3(de, local: int, steps: int, warmup: int) -> dict:
     """The large configuration: 1500x1000, disparities 0-255, 12 BP iterations, thin
     strips and low-texture regions; device-timed, one pair and four pairs a launch."""
@@ -552,6 +595,7 @@ def run_ours(args) -> None:
                        "d2h_bytes_per_step": B * 9 * WH},
                "gpu_launches": 4 * K * ((B + 63) // 64)}
         if ws == 1 and not args.no_extras:
+            out["sparse_c1"] = run_c1(de, local, max(3, K // 2), Wm)
             out["large_c3"] = run_c3(de, local, max(3, K // 4), Wm)
             out["batched_c4"] = run_c4(de, local, K, Wm)
             out["serving_c5"] = run_c5(de, local)

@@ -473,14 +473,16 @@ __device__ __forceinline__ uint32_t pk16(int32_t lo, int32_t hi) {
 // four, and any merge order gives the sequential scan's answer.  The winner's
 // neighbour costs are read back from a per-group row buffer.
 //
-// No block-wide step: each lane reads its own 2*KT bytes of a row straight from global memory, PF rows
-// ahead of use through a register ring (the rows of a warp's columns are adjacent,
-// so a warp's loads and stores of one row are contiguous), and the only
-// synchronisation is the group's own merge of a column's lanes.  Warps therefore
-// run at their own pace instead of meeting at a barrier every row.  A lane reads back
-// only what it stored itself in the forward pass.  KT = 4 gives one column per warp
-// (the most columns in flight, for small batches); 8 and 16 trade columns for
-// disparities per lane.
+// No block-wide step: each lane reads its own 2*KT bytes of a row straight from
+// global memory, PF rows ahead of use through a register ring (the rows of a warp's
+// columns are adjacent, so a warp's loads and stores of one row are contiguous), and
+// the only synchronisation is the group's own merge of a column's lanes.  Warps
+// therefore run at their own pace instead of meeting at a barrier every row.  A lane
+// reads back only what it stored itself in the forward pass.  Only the filter state
+// runs from row to row, so the backward pass merges several rows' keys together
+// (one row buffer each) and their shuffle chains interleave.  KT = 4 gives one
+// column per warp (the most columns in flight, for small batches); 8 and 16 trade
+// columns for disparities per lane.
 template <int KW>   // KW 32-bit words (2*KW disparities) per lane and row
 __device__ __forceinline__ void vload(const uint32_t* p, uint32_t* w) {
   if constexpr (KW == 2) {
@@ -510,10 +512,11 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
   constexpr int KW = KT / 2;                         // 32-bit words per lane and row
   constexpr int NCOL = NT / TPCP;                    // columns per CTA tile
-  // backward rows whose lane merges run together: the whole prefetch ring (8 rows)
-  // where it is 8 deep (at 8 disparities per lane this spills a few bytes of
-  // loop-invariant state and is still the fastest), 2 at 16 disparities per lane
-  constexpr int kRB = KT >= 16 ? 2 : (PF >= 8 ? 8 : 4);   // (PF = 16 keeps 8)
+  // backward rows whose lane merges run together: 8 where the prefetch ring is 8 or
+  // 16 deep (at 8 disparities per lane this spills a few bytes of loop-invariant
+  // state and is still the fastest), 4 with a 4-deep ring, 2 at 16 disparities per
+  // lane (more would spill)
+  constexpr int kRB = KT >= 16 ? 2 : (PF >= 8 ? 8 : 4);
   __shared__ __align__(16) int16_t sbuf[NT / 32][kRB][32 * KT];   // kRB row buffers per warp
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;

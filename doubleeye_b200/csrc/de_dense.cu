@@ -159,18 +159,20 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
   P.ay[size_t(y) * W + x] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
 }
 
-// k_census33x2: the 7x7 census (the default window), two vertically adjacent pixels
-// per thread.  Their windows share six of their seven rows, so each byte read from
-// the shared tile serves both pixels' compares: 56 loads per pixel pair per image
-// instead of 98.  Tiles are 32 x 16 pixels; the bit order, border zeros, packed
-// layout and coefficient planes are those of k_census<3,3>.
-constexpr int kC2Y = 2 * kCTY;                      // tile rows (two per thread)
+// k_census33x: the 7x7 census (the default window), NR vertically adjacent pixels
+// per thread.  Their windows share most of their rows, so each byte read from the
+// shared tile serves up to NR pixels' compares: (6 + NR) x 7 loads per NR pixels per
+// image instead of 49 each.  Tiles are 32 x (8 NR) pixels; the bit order, border
+// zeros, packed layout and coefficient planes are those of k_census<3,3>.
+constexpr int kCensusNR = 4;                        // pixels per thread (rows)
+constexpr int kC2Y = kCensusNR * kCTY;              // tile rows
 
 __host__ __device__ constexpr int census77_bit(int dy, int dx) {  // row-major, no centre
   return (dy + 3) * 7 + (dx + 3) - ((dy > 0 || (dy == 0 && dx > 0)) ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(kCTX * kCTY) k_census33x2(DevCfg cfg, Batch b) {
+__global__ void __launch_bounds__(kCTX * kCTY) k_census33x(DevCfg cfg, Batch b) {
+  constexpr int NR = kCensusNR;
   __shared__ uint8_t sL[kC2Y + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
   __shared__ uint8_t sR[kC2Y + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
   __shared__ uint16_t srf[256];
@@ -193,49 +195,50 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census33x2(DevCfg cfg, Batch b)
     sR[ty][tx] = in ? P.R[gi] : 0;
   }
   __syncthreads();
-  const int x = x0 + threadIdx.x, ya = y0 + 2 * threadIdx.y;
-  if (x >= W || ya >= H) return;
-  const int cx = threadIdx.x + kMaxHalf, cy = 2 * threadIdx.y + kMaxHalf;   // pixel a
-  const uint32_t cla = sL[cy][cx], cra = sR[cy][cx];
-  const uint32_t clb = sL[cy + 1][cx], crb = sR[cy + 1][cx];
-  uint32_t la0 = 0, la1 = 0, ra0 = 0, ra1 = 0, lb0 = 0, lb1 = 0, rb0 = 0, rb1 = 0;
+  const int x = x0 + threadIdx.x, y0t = y0 + NR * threadIdx.y;
+  if (x >= W || y0t >= H) return;
+  const int cx = threadIdx.x + kMaxHalf, cy = NR * threadIdx.y + kMaxHalf;   // first pixel
+  uint32_t cl[NR], cr[NR], l0[NR], l1[NR], r0[NR], r1[NR];
 #pragma unroll
-  for (int w = 0; w < 8; ++w)                        // tile row cy - 3 + w
+  for (int i = 0; i < NR; ++i) {
+    cl[i] = sL[cy + i][cx];
+    cr[i] = sR[cy + i][cx];
+    l0[i] = l1[i] = r0[i] = r1[i] = 0;
+  }
+#pragma unroll
+  for (int w = 0; w < 6 + NR; ++w)                   // tile row cy - 3 + w
 #pragma unroll
     for (int dx = -3; dx <= 3; ++dx) {
       const uint32_t vl = sL[cy - 3 + w][cx + dx], vr = sR[cy - 3 + w][cx + dx];
-      if (w <= 6 && !(w == 3 && dx == 0)) {          // pixel a, dy = w - 3
-        const int bit = census77_bit(w - 3, dx);
-        const uint32_t fl = vl < cla, fr = vr < cra;
-        if (bit < 32) { la0 |= fl << bit; ra0 |= fr << bit; }
-        else { la1 |= fl << (bit - 32); ra1 |= fr << (bit - 32); }
-      }
-      if (w >= 1 && !(w == 4 && dx == 0)) {          // pixel b, dy = w - 4
-        const int bit = census77_bit(w - 4, dx);
-        const uint32_t fl = vl < clb, fr = vr < crb;
-        if (bit < 32) { lb0 |= fl << bit; rb0 |= fr << bit; }
-        else { lb1 |= fl << (bit - 32); rb1 |= fr << (bit - 32); }
+#pragma unroll
+      for (int i = 0; i < NR; ++i) {                 // pixel i sees this row at dy = w - 3 - i
+        const int dy = w - 3 - i;
+        if (dy < -3 || dy > 3 || (dy == 0 && dx == 0)) continue;
+        const int bit = census77_bit(dy, dx);
+        const uint32_t fl = vl < cl[i], fr = vr < cr[i];
+        if (bit < 32) { l0[i] |= fl << bit; r0[i] |= fr << bit; }
+        else { l1[i] |= fl << (bit - 32); r1[i] |= fr << (bit - 32); }
       }
     }
-  auto emit = [&](int y, int cyy, uint32_t l0, uint32_t l1, uint32_t r0, uint32_t r1,
-                  uint32_t cl, uint32_t cr) {
+#pragma unroll
+  for (int i = 0; i < NR; ++i) {
+    const int y = y0t + i, cyy = cy + i;
+    if (y >= H) break;
     uint64_t wl = 0, wr = 0;
     if (x >= 3 && x < W - 3 && y >= 3 && y < H - 3) {
-      wl = (uint64_t(l1) << 32) | l0;
-      wr = (uint64_t(r1) << 32) | r0;
+      wl = (uint64_t(l1[i]) << 32) | l0[i];
+      wr = (uint64_t(r1[i]) << 32) | r0[i];
     }
     if (cfg.packed) {
-      wl |= (uint64_t(kGuard) | (uint64_t(cl) << kPixShift)) << 32;
-      wr |= (uint64_t(cr) << kPixShift) << 32;
+      wl |= (uint64_t(kGuard) | (uint64_t(cl[i]) << kPixShift)) << 32;
+      wr |= (uint64_t(cr[i]) << kPixShift) << 32;
     }
     P.cwL[size_t(y) * P.cpitch + P.lpad + x] = wl;
     P.cwR[size_t(y) * P.cpitch + x] = wr;
-    const int c = int(cl);
+    const int c = int(cl[i]);
     P.ax[size_t(y) * P.apitch + P.lpad + x] = x > 0 ? srf[abs(c - int(sL[cyy][cx - 1]))] : srf[0];
     P.ay[size_t(y) * W + x] = y > 0 ? srf[abs(c - int(sL[cyy - 1][cx]))] : srf[0];
-  };
-  emit(ya, cy, la0, la1, ra0, ra1, cla, cra);
-  if (ya + 1 < H) emit(ya + 1, cy + 1, lb0, lb1, rb0, rb1, clb, crb);
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -1194,14 +1197,14 @@ cudaError_t set_smem(K kernel, size_t bytes) {
 cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int tiles = b.pix_prefix[b.n];
   if (tiles == 0) return cudaSuccess;
-  if (cfg.hw == 3 && cfg.hh == 3) {                   // 32 x 16 tiles of its own
+  if (cfg.hw == 3 && cfg.hh == 3) {                   // 32 x (8 NR) tiles of its own
     thread_local Batch b2;
     b2 = b;
     b2.pix_prefix[0] = 0;
     for (int i = 0; i < b.n; ++i)
       b2.pix_prefix[i + 1] = b2.pix_prefix[i] + ((b.p[i].W + kCTX - 1) / kCTX) *
                                                     ((b.p[i].H + kC2Y - 1) / kC2Y);
-    k_census33x2<<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
+    k_census33x<<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
   }
   else if (cfg.hw == 4 && cfg.hh == 3) k_census<4, 3><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
   else k_census<0, 0><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);

@@ -159,19 +159,23 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
   P.ay[size_t(y) * W + x] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
 }
 
-// k_census33x: the 7x7 census (the default window), NR vertically adjacent pixels
-// per thread.  Their windows share most of their rows, so each byte read from the
-// shared tile serves up to NR pixels' compares: (6 + NR) x 7 loads per NR pixels per
-// image instead of 49 each.  Tiles are 32 x (8 NR) pixels; the bit order, border
-// zeros, packed layout and coefficient planes are those of k_census<3,3>.
+// k_census_rows<HW>: the (2 HW + 1) x 7 census (7x7, the default, and 9x7), NR
+// vertically adjacent pixels per thread.  Their windows share most of their rows, so
+// each byte read from the shared tile serves up to NR pixels' compares: (6 + NR) rows
+// of loads per NR pixels per image instead of 7 rows each.  Tiles are 32 x (8 NR)
+// pixels; the bit order, border zeros, packed layout and coefficient planes are those
+// of k_census<HW,3>.
 constexpr int kCensusNR = 4;                        // pixels per thread (rows)
 constexpr int kC2Y = kCensusNR * kCTY;              // tile rows
 
-__host__ __device__ constexpr int census77_bit(int dy, int dx) {  // row-major, no centre
-  return (dy + 3) * 7 + (dx + 3) - ((dy > 0 || (dy == 0 && dx > 0)) ? 1 : 0);
+template <int HW>
+__host__ __device__ constexpr int census_bit(int dy, int dx) {   // row-major, no centre
+  return (dy + 3) * (2 * HW + 1) + (dx + HW) - ((dy > 0 || (dy == 0 && dx > 0)) ? 1 : 0);
 }
 
-__global__ void __launch_bounds__(kCTX * kCTY) k_census33x(DevCfg cfg, Batch b) {
+template <int HW>
+__global__ void __launch_bounds__(kCTX * kCTY) k_census_rows(DevCfg cfg, Batch b) {
+  static_assert(HW >= 1 && HW <= kMaxHalf, "half-width");
   constexpr int NR = kCensusNR;
   __shared__ uint8_t sL[kC2Y + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
   __shared__ uint8_t sR[kC2Y + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
@@ -208,13 +212,13 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census33x(DevCfg cfg, Batch b) 
 #pragma unroll
   for (int w = 0; w < 6 + NR; ++w)                   // tile row cy - 3 + w
 #pragma unroll
-    for (int dx = -3; dx <= 3; ++dx) {
+    for (int dx = -HW; dx <= HW; ++dx) {
       const uint32_t vl = sL[cy - 3 + w][cx + dx], vr = sR[cy - 3 + w][cx + dx];
 #pragma unroll
       for (int i = 0; i < NR; ++i) {                 // pixel i sees this row at dy = w - 3 - i
         const int dy = w - 3 - i;
         if (dy < -3 || dy > 3 || (dy == 0 && dx == 0)) continue;
-        const int bit = census77_bit(dy, dx);
+        const int bit = census_bit<HW>(dy, dx);
         const uint32_t fl = vl < cl[i], fr = vr < cr[i];
         if (bit < 32) { l0[i] |= fl << bit; r0[i] |= fr << bit; }
         else { l1[i] |= fl << (bit - 32); r1[i] |= fr << (bit - 32); }
@@ -225,7 +229,7 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census33x(DevCfg cfg, Batch b) 
     const int y = y0t + i, cyy = cy + i;
     if (y >= H) break;
     uint64_t wl = 0, wr = 0;
-    if (x >= 3 && x < W - 3 && y >= 3 && y < H - 3) {
+    if (x >= HW && x < W - HW && y >= 3 && y < H - 3) {
       wl = (uint64_t(l1[i]) << 32) | l0[i];
       wr = (uint64_t(r1[i]) << 32) | r0[i];
     }
@@ -1197,17 +1201,18 @@ cudaError_t set_smem(K kernel, size_t bytes) {
 cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int tiles = b.pix_prefix[b.n];
   if (tiles == 0) return cudaSuccess;
-  if (cfg.hw == 3 && cfg.hh == 3) {                   // 32 x (8 NR) tiles of its own
+  if ((cfg.hw == 3 || cfg.hw == 4) && cfg.hh == 3) {  // 32 x (8 NR) tiles of its own
     thread_local Batch b2;
     b2 = b;
     b2.pix_prefix[0] = 0;
     for (int i = 0; i < b.n; ++i)
       b2.pix_prefix[i + 1] = b2.pix_prefix[i] + ((b.p[i].W + kCTX - 1) / kCTX) *
                                                     ((b.p[i].H + kC2Y - 1) / kC2Y);
-    k_census33x<<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
+    if (cfg.hw == 3) k_census_rows<3><<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
+    else k_census_rows<4><<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
+  } else {
+    k_census<0, 0><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
   }
-  else if (cfg.hw == 4 && cfg.hh == 3) k_census<4, 3><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
-  else k_census<0, 0><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
   return cudaGetLastError();
 }
 

@@ -10,6 +10,7 @@
 #include <mutex>
 #include <system_error>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -546,11 +547,17 @@ struct de_ctx {
   de_cfg cfg;
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t copy = nullptr;                       // uploads/downloads beside compute
-  cudaEvent_t ev_in = nullptr, ev_done = nullptr;
+  cudaStream_t copy = nullptr;                       // downloads beside compute
+  cudaStream_t upload = nullptr;                     // uploads beside compute
+  static constexpr int kChunks = 3;                  // most chunks a batch is cut into
+  cudaEvent_t ev_in[kChunks] = {}, ev_done[kChunks] = {};
   void* dws = nullptr;        size_t dws_cap = 0;
   void* dio = nullptr;        size_t dio_cap = 0;    // device images + outputs
   void* hio = nullptr;        size_t hio_cap = 0;    // pinned mirror of dio
+  // Whether a host pointer was page-locked when last asked.  A stale answer only
+  // costs speed: a pageable buffer taken for pinned is copied by the driver's own
+  // staging, a pinned one taken for pageable through the mirror.
+  std::unordered_map<const void*, bool> pinned;
 };
 
 namespace {
@@ -668,8 +675,11 @@ int de_ctx_create(const de_cfg* cfg, int device, de_ctx** out) {
   c->device = device;
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_in, cudaEventDisableTiming);
-  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking);
+  for (int i = 0; i < de_ctx::kChunks && e == cudaSuccess; ++i) {
+    e = cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming);
+  }
   if (e != cudaSuccess) {
     de_ctx_destroy(c);
     return cuda_fail(e, "creating the context's streams and events");
@@ -683,11 +693,15 @@ int de_ctx_destroy(de_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy) cudaStreamSynchronize(c->copy);
+  if (c->upload) cudaStreamSynchronize(c->upload);
   if (c->dws) cudaFree(c->dws);
   if (c->dio) cudaFree(c->dio);
   if (c->hio) cudaFreeHost(c->hio);
-  if (c->ev_in) cudaEventDestroy(c->ev_in);
-  if (c->ev_done) cudaEventDestroy(c->ev_done);
+  for (int i = 0; i < de_ctx::kChunks; ++i) {
+    if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
+    if (c->ev_done[i]) cudaEventDestroy(c->ev_done[i]);
+  }
+  if (c->upload) cudaStreamDestroy(c->upload);
   if (c->copy) cudaStreamDestroy(c->copy);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -716,25 +730,23 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   uint8_t* Hb = static_cast<uint8_t*>(c->hio);
   uint8_t* Db = static_cast<uint8_t*>(c->dio);
   int* hstat = reinterpret_cast<int*>(Hb + plan.end);   // pinned: one status word a chunk
-  hstat[0] = hstat[1] = 0;
+  for (int k = 0; k < de_ctx::kChunks; ++k) hstat[k] = 0;
+  auto is_pinned = [&](const void* p) {
+    auto it = c->pinned.find(p);
+    if (it != c->pinned.end()) return it->second;
+    if (c->pinned.size() >= 4096) c->pinned.clear();
+    return c->pinned[p] = host_pinned(p);
+  };
   // Each host buffer moves by DMA straight from or to the caller's memory when that
   // memory is pinned, else through the context's pinned mirror at the same offset.
   struct Io { void* host; size_t off, bytes; bool pinned; int pair; };
-  std::vector<Io> ins, outs;
   std::vector<de_pair> dp(n);
   size_t out_bytes = 0;
   for (int i = 0; i < n; ++i) {
     const IoLayout& l = plan.p[i];
     const size_t WH = size_t(hp[i].W) * hp[i].H;
-    ins.push_back({const_cast<uint8_t*>(hp[i].L), l.L, WH, host_pinned(hp[i].L), i});
-    ins.push_back({const_cast<uint8_t*>(hp[i].R), l.R, WH, host_pinned(hp[i].R), i});
-    auto out = [&](void* h, size_t off, size_t bytes) {
-      if (h) { outs.push_back({h, off, bytes, host_pinned(h), i}); out_bytes += bytes; }
-    };
-    out(hp[i].disp, l.disp, WH * 4);
-    out(hp[i].margin, l.margin, WH * 4);
-    out(hp[i].conf, l.conf, WH);
-    out(hp[i].cand, l.cand, WH * 24);
+    out_bytes += (hp[i].disp ? WH * 4 : 0) + (hp[i].margin ? WH * 4 : 0) +
+                 (hp[i].conf ? WH : 0) + (hp[i].cand ? WH * 24 : 0);
     dp[i] = hp[i];
     dp[i].L = Db + l.L;
     dp[i].R = Db + l.R;
@@ -743,49 +755,101 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
     dp[i].conf = hp[i].conf ? Db + l.conf : nullptr;
     dp[i].cand = hp[i].cand ? reinterpret_cast<float*>(Db + l.cand) : nullptr;
   }
-  // Two chunks when there is enough to move: the second chunk's upload and the first
-  // chunk's download run on the copy stream while the other chunk computes, so only
-  // the first upload and the (smaller) second download are not hidden.
-  const int n1 = (n >= 4 && out_bytes >= (size_t(8) << 20)) ? (3 * n + 3) / 4 : n;
-  std::vector<HostCopy> jobs;
-  for (const Io& io : ins)
-    if (!io.pinned) jobs.push_back({Hb + io.off, io.host, io.bytes});
-  parallel_copy(jobs);
+  auto inputs = [&](int first, int last) {
+    std::vector<Io> v;
+    for (int i = first; i < last; ++i) {
+      const IoLayout& l = plan.p[i];
+      const size_t WH = size_t(hp[i].W) * hp[i].H;
+      v.push_back({const_cast<uint8_t*>(hp[i].L), l.L, WH, is_pinned(hp[i].L), i});
+      v.push_back({const_cast<uint8_t*>(hp[i].R), l.R, WH, is_pinned(hp[i].R), i});
+    }
+    return v;
+  };
+  auto outputs = [&]() {
+    std::vector<Io> v;
+    for (int i = 0; i < n; ++i) {
+      const IoLayout& l = plan.p[i];
+      const size_t WH = size_t(hp[i].W) * hp[i].H;
+      auto out = [&](void* h, size_t off, size_t bytes) {
+        if (h) v.push_back({h, off, bytes, is_pinned(h), i});
+      };
+      out(hp[i].disp, l.disp, WH * 4);
+      out(hp[i].margin, l.margin, WH * 4);
+      out(hp[i].conf, l.conf, WH);
+      out(hp[i].cand, l.cand, WH * 24);
+    }
+    return v;
+  };
+  auto stage = [&](const std::vector<Io>& v) {          // pageable inputs into the mirror
+    std::vector<HostCopy> jobs;
+    for (const Io& io : v)
+      if (!io.pinned) jobs.push_back({Hb + io.off, io.host, io.bytes});
+    parallel_copy(jobs);
+  };
   auto move = [&](const Io& io, bool up, cudaStream_t st) -> cudaError_t {
     void* h = io.pinned ? io.host : Hb + io.off;
     return up ? cudaMemcpyAsync(Db + io.off, h, io.bytes, cudaMemcpyHostToDevice, st)
               : cudaMemcpyAsync(h, Db + io.off, io.bytes, cudaMemcpyDeviceToHost, st);
   };
+  // Chunks when there is enough to move: chunk k+1's upload (upload stream) and
+  // chunk k's download (download stream) run while another chunk computes, so only
+  // the first upload and the last download are exposed.  Sizes fall off (about 1/2,
+  // 1/3, 1/5 of the batch for three chunks) so each chunk's compute covers the
+  // previous chunk's download.  The first chunk is uploaded and launched before
+  // anything else is prepared.
+  int bound[de_ctx::kChunks + 1] = {0};
+  int nch = 1;
+  if (out_bytes >= (size_t(8) << 20) && n >= 8) {
+    nch = 3;
+    bound[1] = (n + 1) / 2;
+    bound[2] = bound[1] + std::max(1, (n - bound[1]) * 5 / 8);
+  } else if (out_bytes >= (size_t(8) << 20) && n >= 4) {
+    nch = 2;
+    bound[1] = (2 * n + 2) / 3;
+  }
+  bound[nch] = n;
+  std::vector<Io> outs;
   auto enqueue = [&]() -> int {
     int r;
-    for (const Io& io : ins) DE_CUDA(move(io, true, io.pair < n1 ? c->stream : c->copy));
-    if (n1 < n) DE_CUDA(cudaEventRecord(c->ev_in, c->copy));
-    if ((r = de_dense_dev(&c->cfg, dp.data(), n1, c->dws, c->dws_cap, c->stream))) return r;
-    DE_CUDA(cudaMemcpyAsync(&hstat[0], c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    if (n1 < n) {
-      DE_CUDA(cudaEventRecord(c->ev_done, c->stream));
-      DE_CUDA(cudaStreamWaitEvent(c->copy, c->ev_done, 0));
-      for (const Io& io : outs)
-        if (io.pair < n1) DE_CUDA(move(io, false, c->copy));
-      DE_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in, 0));
-      if ((r = de_dense_dev(&c->cfg, dp.data() + n1, n - n1, c->dws, c->dws_cap, c->stream)))
+    const std::vector<Io> in0 = inputs(0, bound[1]);
+    stage(in0);
+    for (const Io& io : in0) DE_CUDA(move(io, true, c->stream));
+    for (int k = 0; k < nch; ++k) {
+      if (k > 0) DE_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
+      if ((r = de_dense_dev(&c->cfg, dp.data() + bound[k], bound[k + 1] - bound[k], c->dws,
+                            c->dws_cap, c->stream)))
         return r;
-      DE_CUDA(cudaMemcpyAsync(&hstat[1], c->dws, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      DE_CUDA(cudaMemcpyAsync(&hstat[k], c->dws, sizeof(int), cudaMemcpyDeviceToHost,
+                              c->stream));
+      DE_CUDA(cudaEventRecord(c->ev_done[k], c->stream));
+      if (k == 0) {                                   // the other chunks' inputs, now
+        for (int j = 1; j < nch; ++j) {
+          const std::vector<Io> in = inputs(bound[j], bound[j + 1]);
+          stage(in);
+          for (const Io& io : in) DE_CUDA(move(io, true, c->upload));
+          DE_CUDA(cudaEventRecord(c->ev_in[j], c->upload));
+        }
+        outs = outputs();
+      }
+      DE_CUDA(cudaStreamWaitEvent(c->copy, c->ev_done[k], 0));
+      for (const Io& io : outs)
+        if (io.pair >= bound[k] && io.pair < bound[k + 1]) DE_CUDA(move(io, false, c->copy));
     }
-    for (const Io& io : outs)
-      if (io.pair >= n1 || n1 == n) DE_CUDA(move(io, false, c->stream));
     return DE_OK;
   };
   // whatever was enqueued finishes before the call returns, on success or not
   rc = enqueue();
   const cudaError_t e1 = cudaStreamSynchronize(c->stream);
   const cudaError_t e2 = cudaStreamSynchronize(c->copy);
+  const cudaError_t e3 = cudaStreamSynchronize(c->upload);
   if (rc) return rc;
   if (e1 != cudaSuccess) return cuda_fail(e1, "cudaStreamSynchronize");
   if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamSynchronize");
-  const int status = hstat[0] ? hstat[0] : hstat[1];
+  if (e3 != cudaSuccess) return cuda_fail(e3, "cudaStreamSynchronize");
+  int status = 0;
+  for (int k = 0; k < nch && !status; ++k) status = hstat[k];
   if (status) return fail(DE_ERR_TIMEOUT, "a bounded device wait ran out (status %d)", status);
-  jobs.clear();
+  std::vector<HostCopy> jobs;
   for (const Io& io : outs)
     if (!io.pinned) jobs.push_back({io.host, Hb + io.off, io.bytes});
   parallel_copy(jobs);

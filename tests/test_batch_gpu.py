@@ -150,3 +150,30 @@ def test_host_batch_pinned_and_pageable_agree(de, batch):
             a, b = getattr(pageable[k], key), getattr(got[k], key)
             assert same(torch.from_numpy(a), torch.from_numpy(b)), (k, key)
             assert same(torch.from_numpy(np.ascontiguousarray(b)), dev[k][key]), (k, key)
+
+
+def test_host_batch_three_chunks_equal_single_pairs(de):
+    """Ten host pairs run as three chunks whose uploads and downloads overlap the other
+    chunks' compute; every pair's outputs equal a call with that pair alone."""
+    from doubleeye_b200 import synth
+    pairs = [synth.slanted_planes(640, 480, 63, seed=k, tag="chunks") for k in range(10)]
+    cfg = de.Cfg(dmax=64, iters=4)
+    shapes = [p.left.shape for p in pairs]
+    host = []
+    for k, p in enumerate(pairs):                       # a mix of pinned and pageable inputs
+        if k % 3 == 0:
+            hl, hr = de.pinned_empty(p.left.shape, np.uint8), de.pinned_empty(p.right.shape, np.uint8)
+            hl[...] = p.left
+            hr[...] = p.right
+            host.append((hl, hr))
+        else:
+            host.append((p.left, p.right))
+    outs = de.new_results(shapes, pinned=True)
+    for k in range(0, 10, 2):                           # and of pinned and pageable outputs
+        outs[k] = de.new_results([shapes[k]], pinned=False)[0]
+    got = de.run_dense_batch(host, cfg, out=outs)
+    for k, p in enumerate(pairs):
+        one = de.run_dense(p.left, p.right, cfg, want_cand=False)
+        for key in ("disp", "margin", "conf"):
+            a, b = getattr(got[k], key), getattr(one, key)
+            assert same(torch.from_numpy(np.ascontiguousarray(a)), torch.from_numpy(b)), (k, key)

@@ -157,6 +157,45 @@ void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc) {
   p->Dpad = dpad_of(D);
 }
 
+// Copies between pageable and pinned host memory, split over a few threads when
+// there is enough to move (one core's memcpy is far below host memory bandwidth).
+void parallel_copy(const std::vector<HostCopy>& jobs) {
+  size_t total = 0;
+  for (const HostCopy& j : jobs) total += j.n;
+  const unsigned hc = std::thread::hardware_concurrency();
+  const int nt = int(std::min<size_t>({8, hc > 1 ? hc / 2 : 1, total >> 22}));
+  if (nt <= 1) {
+    for (const HostCopy& j : jobs) std::memcpy(j.dst, j.src, j.n);
+    return;
+  }
+  // cut every copy into pieces of about total / (4 nt) bytes, dealt round-robin
+  const size_t piece = std::max<size_t>(size_t(1) << 20, total / (4 * size_t(nt)));
+  std::vector<HostCopy> pieces;
+  for (const HostCopy& j : jobs)
+    for (size_t o = 0; o < j.n; o += piece)
+      pieces.push_back({static_cast<uint8_t*>(j.dst) + o, static_cast<const uint8_t*>(j.src) + o,
+                        std::min(piece, j.n - o)});
+  // Worker t copies pieces t, t + nt, ...; the calling thread does the share of any
+  // worker it could not start (no exception leaves this C-ABI path).
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  auto share = [&pieces, nt](int t) {
+    for (size_t k = t; k < pieces.size(); k += nt)
+      std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
+  };
+  int started = 1;
+  for (int t = 1; t < nt; ++t, ++started) {
+    try {
+      th.emplace_back(share, t);
+    } catch (const std::system_error&) {
+      break;
+    }
+  }
+  share(0);
+  for (int t = started; t < nt; ++t) share(t);
+  for (std::thread& t : th) t.join();
+}
+
 }  // namespace de
 
 namespace {
@@ -618,46 +657,6 @@ bool host_pinned(const void* p) {
   return a.type == cudaMemoryTypeHost;
 }
 
-// Copies between pageable and pinned host memory, split over a few threads when
-// there is enough to move (one core's memcpy is far below host memory bandwidth).
-struct HostCopy { void* dst; const void* src; size_t n; };
-void parallel_copy(const std::vector<HostCopy>& jobs) {
-  size_t total = 0;
-  for (const HostCopy& j : jobs) total += j.n;
-  const unsigned hc = std::thread::hardware_concurrency();
-  const int nt = int(std::min<size_t>({8, hc > 1 ? hc / 2 : 1, total >> 22}));
-  if (nt <= 1) {
-    for (const HostCopy& j : jobs) std::memcpy(j.dst, j.src, j.n);
-    return;
-  }
-  // cut every copy into pieces of about total / (4 nt) bytes, dealt round-robin
-  const size_t piece = std::max<size_t>(size_t(1) << 20, total / (4 * size_t(nt)));
-  std::vector<HostCopy> pieces;
-  for (const HostCopy& j : jobs)
-    for (size_t o = 0; o < j.n; o += piece)
-      pieces.push_back({static_cast<uint8_t*>(j.dst) + o, static_cast<const uint8_t*>(j.src) + o,
-                        std::min(piece, j.n - o)});
-  // Worker t copies pieces t, t + nt, ...; the calling thread does the share of any
-  // worker it could not start (no exception leaves this C-ABI path).
-  std::vector<std::thread> th;
-  th.reserve(nt - 1);
-  auto share = [&pieces, nt](int t) {
-    for (size_t k = t; k < pieces.size(); k += nt)
-      std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].n);
-  };
-  int started = 1;
-  for (int t = 1; t < nt; ++t, ++started) {
-    try {
-      th.emplace_back(share, t);
-    } catch (const std::system_error&) {
-      break;
-    }
-  }
-  share(0);
-  for (int t = started; t < nt; ++t) share(t);
-  for (std::thread& t : th) t.join();
-}
-
 }  // namespace
 
 extern "C" {
@@ -781,10 +780,10 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
     return v;
   };
   auto stage = [&](const std::vector<Io>& v) {          // pageable inputs into the mirror
-    std::vector<HostCopy> jobs;
+    std::vector<de::HostCopy> jobs;
     for (const Io& io : v)
       if (!io.pinned) jobs.push_back({Hb + io.off, io.host, io.bytes});
-    parallel_copy(jobs);
+    de::parallel_copy(jobs);
   };
   auto move = [&](const Io& io, bool up, cudaStream_t st) -> cudaError_t {
     void* h = io.pinned ? io.host : Hb + io.off;
@@ -849,10 +848,10 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   int status = 0;
   for (int k = 0; k < nch && !status; ++k) status = hstat[k];
   if (status) return fail(DE_ERR_TIMEOUT, "a bounded device wait ran out (status %d)", status);
-  std::vector<HostCopy> jobs;
+  std::vector<de::HostCopy> jobs;
   for (const Io& io : outs)
     if (!io.pinned) jobs.push_back({io.host, Hb + io.off, io.bytes});
-  parallel_copy(jobs);
+  de::parallel_copy(jobs);
   return DE_OK;
 }
 

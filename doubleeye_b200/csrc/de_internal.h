@@ -5,6 +5,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "../../include/doubleeye_b200.h"
@@ -81,6 +83,11 @@ void make_dev_cfg(const de_cfg& c, DevCfg* out);
 size_t pair_workspace_bytes(int W, int H, int D, bool lrc);
 void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc);
 constexpr size_t kStatusBytes = 256;   // head of every dense workspace
+
+// Host-to-host copies (pageable <-> pinned), split over a few threads when there is
+// enough to move (de_capi.cu).
+struct HostCopy { void* dst; const void* src; size_t n; };
+void parallel_copy(const std::vector<HostCopy>& jobs);
 
 // Launchers (de_dense.cu).  All enqueue on `stream` and return the launch status.
 cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s);

@@ -201,12 +201,13 @@ int launch(de_server* sv, Lane& l) {
   plan_batch(sv, l.batch, &l.slots, &l.in_end, &l.out_begin, &l.out_end, &ws);
   const size_t ws_off = align256(l.out_end);
   std::vector<de_pair> dp(l.batch.size());
+  std::vector<de::HostCopy> jobs;
   for (size_t i = 0; i < l.batch.size(); ++i) {
     Req* r = l.batch[i];
     const Slot& s = l.slots[i];
     const size_t WH = size_t(r->W) * r->H;
-    std::memcpy(l.pin + s.L, r->L.data(), WH);
-    std::memcpy(l.pin + s.R, r->R.data(), WH);
+    jobs.push_back({l.pin + s.L, r->L.data(), WH});
+    jobs.push_back({l.pin + s.R, r->R.data(), WH});
     dp[i] = de_pair{};
     dp[i].L = l.dev + s.L;
     dp[i].R = l.dev + s.R;
@@ -218,6 +219,7 @@ int launch(de_server* sv, Lane& l) {
     dp[i].conf = l.dev + s.conf;
     r->t_launch = now_ms();
   }
+  de::parallel_copy(jobs);
   cudaError_t e = cudaMemcpyAsync(l.dev, l.pin, l.in_end, cudaMemcpyHostToDevice, l.s);
   if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
   int rc = de_dense_dev(&sv->cfg, dp.data(), int(dp.size()), l.dev + ws_off, ws, l.s);
@@ -252,8 +254,18 @@ int launch(de_server* sv, Lane& l) {
     if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "state: %s", cudaGetErrorString(e));
     ++st->frames;
   }
-  e = cudaMemcpyAsync(l.pin + l.out_begin, l.dev + l.out_begin, l.out_end - l.out_begin,
-                      cudaMemcpyDeviceToHost, l.s);
+  // only the planes each request asked for come back
+  for (size_t i = 0; i < l.batch.size() && e == cudaSuccess; ++i) {
+    const Req* r = l.batch[i];
+    const Slot& s = l.slots[i];
+    const size_t WH = size_t(r->W) * r->H;
+    const struct { unsigned bit; size_t off, bytes; } planes[] = {
+        {DE_PLANE_DISP, s.disp, WH * 4}, {DE_PLANE_MARGIN, s.margin, WH * 4},
+        {DE_PLANE_CONF, s.conf, WH}, {DE_PLANE_Q4, s.q4, WH * 2}, {DE_PLANE_QCONF, s.qconf, WH}};
+    for (const auto& pl : planes)
+      if ((r->planes & pl.bit) && e == cudaSuccess)
+        e = cudaMemcpyAsync(l.pin + pl.off, l.dev + pl.off, pl.bytes, cudaMemcpyDeviceToHost, l.s);
+  }
   // the pipeline's status word (set by a bounded device wait that ran out)
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(l.pin + align256(l.out_end), l.dev + ws_off, sizeof(int),

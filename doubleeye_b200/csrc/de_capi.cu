@@ -241,9 +241,6 @@ void fill_batch(const de_cfg& c, const de_pair* pairs, int first, int n, uint8_t
     b->cols_prefix[i + 1] = b->cols_prefix[i] + std::max(0, p.W - 2 * hw - c.dmin);
     b->solve_prefix[i + 1] = b->solve_prefix[i] + p.H;
   }
-  // backward bulk copies of ~4 KB, four deep
-  b->bwd_chunk = std::max(8, 2048 / b->maxDpad);
-  b->bwd_stages = 3;
 }
 
 // Optional stage timing: CUDA events recorded on the launching stream between the

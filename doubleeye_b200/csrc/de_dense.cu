@@ -5,19 +5,24 @@
 // core/tools/de_dense.cpp, core/include/doubleeye/dense_solve.hpp); the work
 // decomposition is this file's own:
 //
-//   k_census  one thread per pixel over a shared-memory tile with halo, both
-//             images at once; writes a 64-bit census word that also carries the
-//             pixel byte (bits 56..63) when the window fits in 48 bits, so the
-//             cost kernel gets Hamming and absolute-difference inputs in one load,
-//             plus the two Q15 coefficient planes of the left image.
+//   k_census_rows / k_census_generic
+//             shared-memory tiles with a halo, both images at once; a thread owns
+//             four vertically adjacent pixels, whose windows share rows (7x7 and
+//             9x7), or one pixel (other windows).  Writes a 64-bit census word that
+//             also carries the pixel byte (bits 52..59) when the window fits in 48
+//             bits, so the cost kernel gets Hamming and absolute-difference inputs
+//             in one load, plus the two Q15 coefficient planes of the left image.
 //   k_rows    one CTA per image row, a thread per PAIR of adjacent disparities
 //             (int16x2 in one 32-bit register): graded score fused with the
 //             horizontal forward pass, then the backward pass, both sequential in
 //             x as integer rounding demands; the row's census words live in
-//             shared memory, the forward result round-trips through L2.
-//   k_cols    one warp per image column, lanes over disparity pairs: vertical
+//             shared memory, the forward result comes back through a ring of bulk
+//             copies.
+//   k_cols    a column is a group of lanes, each lane KT disparities: vertical
 //             forward pass written in place, vertical backward pass fused with the
-//             top-2 (packed-key warp reduction) and the winner's neighbour costs.
+//             top-2 (packed keys, a butterfly over the group) and the winner's
+//             neighbour costs; rows stream through per-lane register rings, with
+//             no block-wide step.
 //   k_solve   one CTA per row: candidate buckets by right pixel, damped max-sum
 //             iterations, belief, and the one-to-one claim done in parallel as a
 //             per-right-pixel arg-max (each pixel claims exactly one right pixel,
@@ -65,7 +70,7 @@ __device__ __forceinline__ int32_t lo16(uint32_t v) { return int32_t(int16_t(v &
 __device__ __forceinline__ int32_t hi16(uint32_t v) { return int32_t(int16_t(v >> 16)); }
 
 // ---------------------------------------------------------------------------------
-// k_census: census words + coefficient planes.
+// Census words + coefficient planes.
 // core/tools/de_dense.cpp:94-129,186-227 (census), :531-561 (rf_coeffs).
 constexpr int kCTX = 32, kCTY = 8, kMaxHalf = 4;
 
@@ -77,27 +82,6 @@ constexpr int kCTX = 32, kCTY = 8, kMaxHalf = 4;
 constexpr uint32_t kCensusHiMask = 0xFFFFu;
 constexpr uint32_t kGuard = 1u << 19;
 constexpr int kPixShift = 20;
-
-template <int HW, int HH>
-__device__ __forceinline__ void census_pair(const uint8_t (*sL)[kCTX + 2 * kMaxHalf],
-                                            const uint8_t (*sR)[kCTX + 2 * kMaxHalf], int cx,
-                                            int cy, uint64_t& wl, uint64_t& wr) {
-  const uint8_t cl = sL[cy][cx], cr = sR[cy][cx];
-  uint32_t l0 = 0, l1 = 0, r0 = 0, r1 = 0;
-  int bit = 0;
-#pragma unroll
-  for (int dy = -HH; dy <= HH; ++dy)
-#pragma unroll
-    for (int dx = -HW; dx <= HW; ++dx) {
-      if (dx == 0 && dy == 0) continue;
-      const uint32_t bl = sL[cy + dy][cx + dx] < cl, br = sR[cy + dy][cx + dx] < cr;
-      if (bit < 32) { l0 |= bl << bit; r0 |= br << bit; }
-      else { l1 |= bl << (bit - 32); r1 |= br << (bit - 32); }
-      ++bit;
-    }
-  wl = (uint64_t(l1) << 32) | l0;
-  wr = (uint64_t(r1) << 32) | r0;
-}
 
 __device__ __forceinline__ void census_generic(const uint8_t (*sL)[kCTX + 2 * kMaxHalf],
                                                const uint8_t (*sR)[kCTX + 2 * kMaxHalf],
@@ -115,8 +99,8 @@ __device__ __forceinline__ void census_generic(const uint8_t (*sL)[kCTX + 2 * kM
     }
 }
 
-template <int HW, int HH>   // HW = 0: runtime window
-__global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
+// Any window up to 9x9 (runtime half-widths), one pixel a thread.
+__global__ void __launch_bounds__(kCTX * kCTY) k_census_generic(DevCfg cfg, Batch b) {
   __shared__ uint8_t sL[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
   __shared__ uint8_t sR[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
   __shared__ uint16_t srf[256];
@@ -141,13 +125,11 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
   __syncthreads();
   const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
   if (x >= W || y >= H) return;
-  const int hw = HW ? HW : cfg.hw, hh = HW ? HH : cfg.hh;
+  const int hw = cfg.hw, hh = cfg.hh;
   const int cx = threadIdx.x + kMaxHalf, cy = threadIdx.y + kMaxHalf;
   uint64_t wl = 0, wr = 0;
-  if (x >= hw && x < W - hw && y >= hh && y < H - hh) {
-    if (HW) census_pair<HW, HH>(sL, sR, cx, cy, wl, wr);
-    else census_generic(sL, sR, cx, cy, hw, hh, wl, wr);
-  }
+  if (x >= hw && x < W - hw && y >= hh && y < H - hh)
+    census_generic(sL, sR, cx, cy, hw, hh, wl, wr);
   if (cfg.packed) {
     wl |= (uint64_t(kGuard) | (uint64_t(sL[cy][cx]) << kPixShift)) << 32;
     wr |= (uint64_t(sR[cy][cx]) << kPixShift) << 32;
@@ -164,7 +146,7 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census(DevCfg cfg, Batch b) {
 // each byte read from the shared tile serves up to NR pixels' compares: (6 + NR) rows
 // of loads per NR pixels per image instead of 7 rows each.  Tiles are 32 x (8 NR)
 // pixels; the bit order, border zeros, packed layout and coefficient planes are those
-// of k_census<HW,3>.
+// of k_census_generic.
 constexpr int kCensusNR = 4;                        // pixels per thread (rows)
 constexpr int kC2Y = kCensusNR * kCTY;              // tile rows
 
@@ -1211,7 +1193,7 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
     if (cfg.hw == 3) k_census_rows<3><<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
     else k_census_rows<4><<<b2.pix_prefix[b.n], dim3(kCTX, kCTY), 0, s>>>(cfg, b2);
   } else {
-    k_census<0, 0><<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
+    k_census_generic<<<tiles, dim3(kCTX, kCTY), 0, s>>>(cfg, b);
   }
   return cudaGetLastError();
 }

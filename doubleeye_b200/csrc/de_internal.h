@@ -65,8 +65,6 @@ struct DevCfg {
 struct Batch {
   int n;
   int maxDpad;
-  int bwd_chunk;       // row kernel: x columns per backward bulk copy
-  int bwd_stages;      // ... ring depth
   int* err;            // device status word (bounded waits that ran out set it)
   int rows_prefix[kMaxBatch + 1];   // row-kernel work items (rows in [hh, H-hh))
   int cols_prefix[kMaxBatch + 1];   // column-kernel work items (cols with candidates)

@@ -7,7 +7,8 @@ onto the GPU, so every setting gives bit-identical results:
   cols_kt           column-kernel tile shape: disparities per lane (0 = by batch size)
   cols_pf           column-kernel prefetch depth: image rows loaded ahead of use
   cols_cta          column-kernel threads per CTA (0 = by batch size)
-  solve_threads     threads per row in the row solve (the BP schedule's width)
+  solve_threads     threads per row in the row solve, the BP schedule's width (0 = by
+                    row width)
 
 ``tune`` times a batch under a coordinate-descent search over these values (CUDA
 events, warm-up first) and returns the fastest setting; ``Tuner`` caches the choice
@@ -27,7 +28,7 @@ KNOBS = {
     "cols_kt": [0, 4, 8, 16],
     "cols_pf": [0, 4, 8, 16],
     "cols_cta": [0, 128, 256],
-    "solve_threads": [128, 256, 512],
+    "solve_threads": [0, 128, 256, 512],
 }
 CACHE = os.path.join(_lib.PKG, "_lib", "autotune.json")
 

@@ -1200,7 +1200,7 @@ cudaError_t launch_census(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
 
 struct de_cfg_hw { int hw, dmin; };
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
-int g_solve_threads = 256;        // threads per row in the solve
+int g_solve_threads = 0;          // threads per row in the solve: 128, 256, 512, 0 = by width
 int g_cols_pf = 0;                // rows the column kernel prefetches: 4, 8, 16, 0 = by shape
 
 template <bool PACKED, int TS, int G>
@@ -1256,7 +1256,7 @@ cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   return cudaSuccess;
 }
 
-void set_solve_threads(int v) { g_solve_threads = (v == 128 || v == 512) ? v : 256; }
+void set_solve_threads(int v) { g_solve_threads = (v == 128 || v == 256 || v == 512) ? v : 0; }
 int get_solve_threads() { return g_solve_threads; }
 void set_rows_ctas_per_sm(int v) { g_rows_ctas_per_sm = v < 1 ? 1 : v; }
 int get_rows_ctas_per_sm() { return g_rows_ctas_per_sm; }
@@ -1317,8 +1317,8 @@ int get_cols_kt() { return g_cols_kt; }
 // Disparities per lane KT; lanes per column Dpad/KT rounded up to a power of two.
 // By default KT = 4 for batches too small to fill the GPU with columns (one column
 // per warp, the most columns in flight), else KT = 8.  KT = 4 needs Dpad <= 128 (32
-// lanes), KT = 16 needs Dpad >= 128.
-cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+// lanes), KT = 16 needs Dpad >= 128.  `b` holds pairs of one disparity group.
+cudaError_t launch_cols_g(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   if (b.cols_prefix[b.n] == 0) return cudaSuccess;
   const de_cfg_hw hwc{cfg.hw, cfg.dmin};
   const long work = long(b.cols_prefix[b.n]) * b.maxDpad;
@@ -1343,7 +1343,34 @@ cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   }
 }
 
-cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref, cudaStream_t s) {
+// One launch per disparity group present in the batch (Dpad = 64 G), so a pair's
+// column groups are sized for its own Dpad rather than the batch's largest, and each
+// group picks its tile shape from its own work.
+cudaError_t launch_cols(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
+  if (b.cols_prefix[b.n] == 0) return cudaSuccess;
+  thread_local Batch sub;
+  for (int G = 1; G <= 4; ++G) {
+    sub = b;
+    sub.n = 0;
+    sub.cols_prefix[0] = 0;
+    sub.maxDpad = 64 * G;
+    for (int i = 0; i < b.n; ++i) {
+      if (b.p[i].Dpad != 64 * G) continue;
+      sub.p[sub.n] = b.p[i];
+      sub.cols_prefix[sub.n + 1] = sub.cols_prefix[sub.n] + (b.cols_prefix[i + 1] - b.cols_prefix[i]);
+      ++sub.n;
+    }
+    if (sub.n == 0) continue;
+    const cudaError_t e = launch_cols_g(cfg, sub, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// `b` holds pairs of one width class.  Shared memory is sized for the class's widest
+// row; threads per row come from the knob, or by width (512 above 1024 pixels, else
+// 256).
+cudaError_t launch_solve_w(const DevCfg& cfg, const Batch& b, bool from_ref, cudaStream_t s) {
   const int items = b.solve_prefix[b.n];
   if (items == 0) return cudaSuccess;
   int maxW = 0;
@@ -1356,13 +1383,39 @@ cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref, cudaS
     kern<<<items, nt, sm, s>>>(cfg, b);
     return cudaSuccess;
   };
-  switch (g_solve_threads) {
+  const int nt = g_solve_threads ? g_solve_threads : (maxW > 1024 ? 512 : 256);
+  switch (nt) {
     case 128: e = from_ref ? go(k_solve<true, 128>, 128) : go(k_solve<false, 128>, 128); break;
     case 512: e = from_ref ? go(k_solve<true, 512>, 512) : go(k_solve<false, 512>, 512); break;
     default: e = from_ref ? go(k_solve<true, 256>, 256) : go(k_solve<false, 256>, 256); break;
   }
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
+}
+
+// One launch per width class (up to 512, up to 1024, wider): the shared-memory
+// working set grows with the row, so a narrow pair launched beside a wide one would
+// run at the wide pair's occupancy.
+cudaError_t launch_solve(const DevCfg& cfg, const Batch& b, bool from_ref, cudaStream_t s) {
+  if (b.solve_prefix[b.n] == 0) return cudaSuccess;
+  thread_local Batch sub;
+  constexpr int kLimit[3] = {512, 1024, 1 << 30};
+  for (int c = 0; c < 3; ++c) {
+    const int lo = c ? kLimit[c - 1] : 0;
+    sub = b;
+    sub.n = 0;
+    sub.solve_prefix[0] = 0;
+    for (int i = 0; i < b.n; ++i) {
+      if (b.p[i].W <= lo || b.p[i].W > kLimit[c]) continue;
+      sub.p[sub.n] = b.p[i];
+      sub.solve_prefix[sub.n + 1] = sub.solve_prefix[sub.n] + (b.solve_prefix[i + 1] - b.solve_prefix[i]);
+      ++sub.n;
+    }
+    if (sub.n == 0) continue;
+    const cudaError_t e = launch_solve_w(cfg, sub, from_ref, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s) {

@@ -179,8 +179,9 @@ DE_API int de_int_probe(int op, int trips, void* stream, float* ms, double* lane
  *   "cols_cta"          column-kernel threads per CTA: 128, 256, or 0 to choose by
  *                       batch size (default 0: 128 for batches of a few 848x480
  *                       pairs or less, else 256)
- *   "solve_threads"     threads per image row in the row solve: 128, 256 or 512
- *                       (default 256) */
+ *   "solve_threads"     threads per image row in the row solve: 128, 256, 512, or
+ *                       0 to choose by row width (default 0: 512 for rows wider
+ *                       than 1024 pixels, else 256) */
 DE_API int de_set_param(const char* name, int value);
 DE_API int de_get_param(const char* name, int* value);
 

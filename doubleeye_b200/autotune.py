@@ -67,9 +67,14 @@ def _time(run, reps: int, warmup: int) -> float:
 
 def tune(run, reps: int = 3, warmup: int = 2, rounds: int = 2) -> tuple[dict, float]:
     """Coordinate descent from the current setting: for each knob in turn keep the
-    fastest value, two rounds.  ``run`` enqueues one batch.  Leaves the best setting
-    applied and returns it with its time (ms per batch)."""
-    best = current()
+    fastest value, two rounds.  ``run`` enqueues one batch.  A winner that differs
+    from the starting setting is then timed against it in alternation (the clock and
+    the memory system drift by a percent or two within a run, so one short timing
+    per trial can pick a setting that is not faster) and kept only if it is at least
+    1% faster there.  Leaves the chosen setting applied and returns it with its time
+    (ms per batch)."""
+    start = current()
+    best = dict(start)
     apply(best)
     best_ms = _time(run, reps, warmup)
     for _ in range(rounds):
@@ -86,6 +91,17 @@ def tune(run, reps: int = 3, warmup: int = 2, rounds: int = 2) -> tuple[dict, fl
             apply(best)
         if not improved:
             break
+    if best != start:
+        t_start = t_best = 0.0
+        for _ in range(2):
+            apply(start)
+            t_start += _time(run, reps, 1)
+            apply(best)
+            t_best += _time(run, reps, 1)
+        if t_best > 0.99 * t_start:
+            best, best_ms = start, t_start / 2
+        else:
+            best_ms = t_best / 2
     apply(best)
     return best, best_ms
 

@@ -599,13 +599,16 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   const int x = xbase + gi;
   const int k0 = sub * KT;
   const bool colok = gi < ncols;
-  const bool live = colok && k0 < Dpad;
   const int kmax = colok ? min(D - 1, x - hw - dmin) : -1;
+  // A lane whose disparities all lie past kmax (the left-edge triangle, or past D)
+  // feeds neither a key nor a neighbour cost, so it is not live.
+  const bool live = colok && k0 < Dpad && k0 <= kmax;
   const int nvalid = max(0, min(KT, kmax - k0 + 1));
   const int yin = H - hh;                             // rows >= yin have zero input
   const size_t grs = size_t(W) * Dpad / 2;            // image-row stride in words
-  // Every lane reads a valid address (lanes without a column or past Dpad read one
-  // they never use), so the loads need no guard; only live lanes store.
+  // Every lane reads a valid address, so the loads need no guard: a lane that is not
+  // live reads its group's first lane's words (the same sectors, no extra traffic)
+  // and never uses them; only live lanes store.
   uint32_t* gcol = reinterpret_cast<uint32_t*>(P.vol + size_t(colok ? x : xbase) * Dpad +
                                                (live ? k0 : 0));
   const uint16_t* ay = P.ay + (colok ? x : xbase);

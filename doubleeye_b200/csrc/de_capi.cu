@@ -585,7 +585,9 @@ struct de_ctx {
   cudaStream_t stream = nullptr;
   cudaStream_t copy = nullptr;                       // downloads beside compute
   cudaStream_t upload = nullptr;                     // uploads beside compute
-  static constexpr int kChunks = 3;                  // most chunks a batch is cut into
+  static constexpr int kChunks = 5;                  // most chunks a batch is cut into
+  // compute streams of a chunked batch, priority falling with the chunk's order
+  cudaStream_t cs[kChunks] = {};
   cudaEvent_t ev_in[kChunks] = {}, ev_done[kChunks] = {};
   void* dws = nullptr;        size_t dws_cap = 0;
   void* dio = nullptr;        size_t dio_cap = 0;    // device images + outputs
@@ -672,6 +674,10 @@ int de_ctx_create(const de_cfg* cfg, int device, de_ctx** out) {
   cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->upload, cudaStreamNonBlocking);
+  int least = 0, greatest = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  for (int i = 0; i < de_ctx::kChunks && e == cudaSuccess; ++i)   // greatest is the lowest number
+    e = cudaStreamCreateWithPriority(&c->cs[i], cudaStreamNonBlocking, std::min(greatest + i, least));
   for (int i = 0; i < de_ctx::kChunks && e == cudaSuccess; ++i) {
     e = cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done[i], cudaEventDisableTiming);
@@ -690,6 +696,8 @@ int de_ctx_destroy(de_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->copy) cudaStreamSynchronize(c->copy);
   if (c->upload) cudaStreamSynchronize(c->upload);
+  for (int i = 0; i < de_ctx::kChunks; ++i)
+    if (c->cs[i]) cudaStreamSynchronize(c->cs[i]);
   if (c->dws) cudaFree(c->dws);
   if (c->dio) cudaFree(c->dio);
   if (c->hio) cudaFreeHost(c->hio);
@@ -697,6 +705,8 @@ int de_ctx_destroy(de_ctx* c) {
     if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
     if (c->ev_done[i]) cudaEventDestroy(c->ev_done[i]);
   }
+  for (int i = 0; i < de_ctx::kChunks; ++i)
+    if (c->cs[i]) cudaStreamDestroy(c->cs[i]);
   if (c->upload) cudaStreamDestroy(c->upload);
   if (c->copy) cudaStreamDestroy(c->copy);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -720,7 +730,6 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   size_t ws = 0;
   if ((rc = de_dense_workspace_bytes(&c->cfg, hp, n, &ws))) return rc;
   const IoPlan plan = io_plan(hp, n);
-  if ((rc = grow_dev(&c->dws, &c->dws_cap, ws))) return rc;
   if ((rc = grow_dev(&c->dio, &c->dio_cap, plan.end))) return rc;
   if ((rc = grow_host(&c->hio, &c->hio_cap, plan.end + kAlign))) return rc;
   uint8_t* Hb = static_cast<uint8_t*>(c->hio);
@@ -789,35 +798,50 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   };
   // Chunks when there is enough to move: chunk k+1's upload (upload stream) and
   // chunk k's download (download stream) run while another chunk computes, so only
-  // the first upload and the last download are exposed.  Sizes fall off (about 1/2,
-  // 1/3, 1/5 of the batch for three chunks) so each chunk's compute covers the
-  // previous chunk's download.  The first chunk is uploaded and launched before
-  // anything else is prepared.
+  // the first upload and the last download are exposed.  Each chunk computes on its
+  // own stream in its own workspace slice, at a priority below the chunk before it:
+  // the first chunk runs as if alone and the later ones take the SMs it leaves idle
+  // (its tails, its lightly occupied kernels), so chunking costs little device
+  // efficiency.  Five chunks from 8 pairs up: small ends (n/8 pairs each) keep the
+  // exposed first upload and last download short, and three equal middle chunks
+  // finish one after another so their downloads overlap the compute behind them
+  // (16 pairs of 848x480: 2, 4, 4, 4, 2).  The first chunk is uploaded and launched
+  // before anything else is prepared.
   int bound[de_ctx::kChunks + 1] = {0};
   int nch = 1;
   if (out_bytes >= (size_t(8) << 20) && n >= 8) {
-    nch = 3;
-    bound[1] = (n + 1) / 2;
-    bound[2] = bound[1] + std::max(1, (n - bound[1]) * 5 / 8);
+    const int e = std::max(1, n / 8), mid = n - 2 * e;
+    const int sizes[5] = {e, (mid + 2) / 3, (mid + 1) / 3, mid / 3, e};
+    nch = 5;
+    for (int k = 0; k < nch; ++k) bound[k + 1] = bound[k] + sizes[k];
   } else if (out_bytes >= (size_t(8) << 20) && n >= 4) {
     nch = 2;
     bound[1] = (2 * n + 2) / 3;
   }
   bound[nch] = n;
+  size_t woff[de_ctx::kChunks + 1] = {0};
+  for (int k = 0; k < nch; ++k) {
+    size_t wk = 0;
+    if ((rc = de_dense_workspace_bytes(&c->cfg, hp + bound[k], bound[k + 1] - bound[k], &wk)))
+      return rc;
+    woff[k + 1] = woff[k] + wk;
+  }
+  if ((rc = grow_dev(&c->dws, &c->dws_cap, std::max(ws, woff[nch])))) return rc;
+  uint8_t* dws = static_cast<uint8_t*>(c->dws);
   std::vector<Io> outs;
   auto enqueue = [&]() -> int {
     int r;
     const std::vector<Io> in0 = inputs(0, bound[1]);
     stage(in0);
-    for (const Io& io : in0) DE_CUDA(move(io, true, c->stream));
+    for (const Io& io : in0) DE_CUDA(move(io, true, c->cs[0]));
     for (int k = 0; k < nch; ++k) {
-      if (k > 0) DE_CUDA(cudaStreamWaitEvent(c->stream, c->ev_in[k], 0));
-      if ((r = de_dense_dev(&c->cfg, dp.data() + bound[k], bound[k + 1] - bound[k], c->dws,
-                            c->dws_cap, c->stream)))
+      cudaStream_t sk = c->cs[k];
+      if (k > 0) DE_CUDA(cudaStreamWaitEvent(sk, c->ev_in[k], 0));
+      if ((r = de_dense_dev(&c->cfg, dp.data() + bound[k], bound[k + 1] - bound[k],
+                            dws + woff[k], woff[k + 1] - woff[k], sk)))
         return r;
-      DE_CUDA(cudaMemcpyAsync(&hstat[k], c->dws, sizeof(int), cudaMemcpyDeviceToHost,
-                              c->stream));
-      DE_CUDA(cudaEventRecord(c->ev_done[k], c->stream));
+      DE_CUDA(cudaMemcpyAsync(&hstat[k], dws + woff[k], sizeof(int), cudaMemcpyDeviceToHost, sk));
+      DE_CUDA(cudaEventRecord(c->ev_done[k], sk));
       if (k == 0) {                                   // the other chunks' inputs, now
         for (int j = 1; j < nch; ++j) {
           const std::vector<Io> in = inputs(bound[j], bound[j + 1]);
@@ -835,7 +859,11 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
   };
   // whatever was enqueued finishes before the call returns, on success or not
   rc = enqueue();
-  const cudaError_t e1 = cudaStreamSynchronize(c->stream);
+  cudaError_t e1 = cudaSuccess;
+  for (int k = 0; k < de_ctx::kChunks; ++k) {
+    const cudaError_t ek = cudaStreamSynchronize(c->cs[k]);
+    if (e1 == cudaSuccess) e1 = ek;
+  }
   const cudaError_t e2 = cudaStreamSynchronize(c->copy);
   const cudaError_t e3 = cudaStreamSynchronize(c->upload);
   if (rc) return rc;

@@ -397,12 +397,13 @@ DE_API int de_dedd_encode_dev(const float* disp, const uint8_t* conf, int W, int
                               int16_t* q4, uint8_t* qconf, void* stream);
 
 /* ---- dense, host pointers, context-owned memory, synchronous ----------------- */
-/* A context owns device buffers, a page-locked mirror and three streams; one thread
+/* A context owns device buffers, a page-locked mirror and its streams; one thread
  * uses it at a time (give each thread its own).  Host buffers may be pageable or
  * page-locked: page-locked ones move by DMA directly, pageable ones through the
- * mirror.  A batch with enough output runs as up to three chunks whose uploads and
- * downloads overlap the other chunks' compute; every call has finished its copies
- * when it returns. */
+ * mirror.  A batch with enough output runs as up to five chunks, each on its own
+ * compute stream (priority falling with the chunk's order) and workspace slice,
+ * whose uploads and downloads overlap the other chunks' compute; every call has
+ * finished its copies when it returns. */
 
 typedef struct de_ctx de_ctx;
 DE_API int de_ctx_create(const de_cfg* cfg, int device, de_ctx** out);

@@ -152,9 +152,10 @@ def test_host_batch_pinned_and_pageable_agree(de, batch):
             assert same(torch.from_numpy(np.ascontiguousarray(b)), dev[k][key]), (k, key)
 
 
-def test_host_batch_three_chunks_equal_single_pairs(de):
-    """Ten host pairs run as three chunks whose uploads and downloads overlap the other
-    chunks' compute; every pair's outputs equal a call with that pair alone."""
+def test_host_batch_chunks_equal_single_pairs(de):
+    """Ten host pairs run as five chunks (1, 3, 3, 2, 1 pairs), each on its own stream
+    and workspace slice, with uploads and downloads overlapping the other chunks'
+    compute; every pair's outputs equal a call with that pair alone."""
     from doubleeye_b200 import synth
     pairs = [synth.slanted_planes(640, 480, 63, seed=k, tag="chunks") for k in range(10)]
     cfg = de.Cfg(dmax=64, iters=4)

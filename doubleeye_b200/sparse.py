@@ -108,28 +108,37 @@ class SparseMatcher:
         """-> (keypoints (kp_cap, 4) f32 tensor, count int32 tensor of 1) on the device."""
         torch = _torch()
         img = _dev_u8(img, self.device)
+        kp = torch.empty((self.kp_cap, 4), dtype=torch.float32, device=self.device)
+        n = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._detect_into(img, kp, n, self._det_ws(img, ws_key), stream)
+        return kp, n
+
+    def _det_ws(self, img, ws_key: str):
         H, W = img.shape
         need = C.c_size_t()
         check(lib().de_detect_workspace_bytes(W, H, C.byref(self.det), C.byref(need)))
-        ws = self._buf(ws_key, need.value)
-        kp = torch.empty((self.kp_cap, 4), dtype=torch.float32, device=self.device)
-        n = torch.zeros(1, dtype=torch.int32, device=self.device)
+        return self._buf(ws_key, need.value), need.value
+
+    def _detect_into(self, img, kp, n, ws, stream):
+        H, W = img.shape
+        buf, nbytes = ws
         check(lib().de_detect_fast_dev(img.data_ptr(), W, H, C.byref(self.det), kp.data_ptr(),
-                                       self.kp_cap, n.data_ptr(), ws.data_ptr(), need.value,
+                                       kp.shape[0], n.data_ptr(), buf.data_ptr(), nbytes,
                                        _stream_handle(stream)))
-        return kp, n
 
     def census_at(self, img, kp, n=None, stream=None):
         """Descriptors (int64 tensor of uint64 bit patterns) at the keypoints."""
         torch = _torch()
         img = _dev_u8(img, self.device)
+        desc = torch.zeros(kp.shape[0], dtype=torch.int64, device=self.device)
+        self._census_into(img, kp, n, desc, stream)
+        return desc
+
+    def _census_into(self, img, kp, n, desc, stream):
         H, W = img.shape
-        cap = kp.shape[0]
-        desc = torch.zeros(cap, dtype=torch.int64, device=self.device)
-        check(lib().de_census_at_dev(img.data_ptr(), W, H, kp.data_ptr(), cap,
+        check(lib().de_census_at_dev(img.data_ptr(), W, H, kp.data_ptr(), kp.shape[0],
                                      n.data_ptr() if n is not None else None, self.hw,
                                      self.hh, desc.data_ptr(), None, _stream_handle(stream)))
-        return desc
 
     def match(self, kl, dl, kr, dr, nl=None, nr=None, stream=None):
         """-> (matches (cap, 7) int32 tensor holding de_match records, count tensor,
@@ -151,13 +160,37 @@ class SparseMatcher:
         return out, n, st
 
     def match_pair(self, L, R, stream=None) -> dict:
-        """Detect both images, describe, match; all on the device, nothing synchronised."""
-        kl, nl = self.detect(L, stream, "detL")
-        kr, nr = self.detect(R, stream, "detR")
-        dl = self.census_at(L, kl, nl, stream)
-        dr = self.census_at(R, kr, nr, stream)
-        m, n, st = self.match(kl, dl, kr, dr, nl, nr, stream)
+        """Detect both images, describe, match; all on the device, nothing synchronised.
+        The right image is detected and described on a second stream beside the left
+        one (the two are independent and each is a few small kernels), and the match
+        waits for both."""
+        torch = _torch()
+        main = stream if stream is not None else torch.cuda.current_stream(self.device)
+        side = self._side_stream()
+        with torch.cuda.stream(main):
+            # everything the side stream touches is allocated (and zeroed) on the main
+            # stream before the fork, so no tensor crosses the allocator's streams
+            L = _dev_u8(L, self.device)
+            R = _dev_u8(R, self.device)
+            kr = torch.empty((self.kp_cap, 4), dtype=torch.float32, device=self.device)
+            nr = torch.zeros(1, dtype=torch.int32, device=self.device)
+            dr = torch.zeros(self.kp_cap, dtype=torch.int64, device=self.device)
+            wsr = self._det_ws(R, "detR")
+            side.wait_stream(main)
+            self._detect_into(R, kr, nr, wsr, side)
+            self._census_into(R, kr, nr, dr, side)
+            kl, nl = self.detect(L, main, "detL")
+            dl = self.census_at(L, kl, nl, main)
+            main.wait_stream(side)
+            m, n, st = self.match(kl, dl, kr, dr, nl, nr, main)
         return dict(kl=kl, nl=nl, kr=kr, nr=nr, dl=dl, dr=dr, matches=m, n=n, stats=st)
+
+    def _side_stream(self):
+        torch = _torch()
+        s = getattr(self, "_side", None)
+        if s is None:
+            s = self._side = torch.cuda.Stream(self.device)
+        return s
 
     # -- host results ---------------------------------------------------------------------
     @staticmethod

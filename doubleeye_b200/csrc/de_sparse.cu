@@ -157,7 +157,7 @@ __device__ float local_std7(const uint8_t* __restrict__ img, int W, int H, int x
 // Detector workspace, carved from one caller allocation.
 struct DetWs {
   float* resp;        // [H*W] response at candidates
-  uint8_t* state;     // [H*W] 0 none, 1 undecided, 2 kept, 3 suppressed
+  uint8_t* state;     // [H*W + 32] 0 none, 1 undecided, 2 kept, 3 suppressed
   int* listA;         // [H*W] candidate pixel indices
   int* listB;         // [H*W]
   int* counters;      // [0] candidates, [1] error
@@ -168,7 +168,7 @@ struct DetWs {
 size_t det_ws_bytes(int W, int H, int cells, int keep) {
   const size_t px = size_t(W) * H;
   auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-  return up(px * 4) + up(px) + 2 * up(px * 4) + up(64) + up(size_t(cells) * keep * 16) +
+  return up(px * 4) + up(px + 32) + 2 * up(px * 4) + up(64) + up(size_t(cells) * keep * 16) +
          up(size_t(cells) * 4);
 }
 
@@ -178,7 +178,7 @@ DetWs carve_det(void* ws, int W, int H, int cells, int keep) {
   uint8_t* p = static_cast<uint8_t*>(ws);
   DetWs d;
   d.resp = reinterpret_cast<float*>(p);           p += up(px * 4);
-  d.state = p;                                    p += up(px);
+  d.state = p;                                    p += up(px + 32);   // word reads past the end
   d.listA = reinterpret_cast<int*>(p);            p += up(px * 4);
   d.listB = reinterpret_cast<int*>(p);            p += up(px * 4);
   d.counters = reinterpret_cast<int*>(p);         p += up(64);
@@ -262,6 +262,78 @@ __global__ void __launch_bounds__(256) k_nms(int W, int H, int rad, DetWs d) {
             if (!stronger(d.resp[j], j, r, t)) continue;
             if (s == 2) { supp = true; break; }
             pend = j;
+          }
+        }
+        if (supp) { st[t] = 3; --sp; continue; }
+        if (pend < 0) { st[t] = 2; --sp; continue; }
+        if (sp == kNmsStack) {              // keep the deeper half; the rest is redone
+#pragma unroll
+          for (int k = 0; k < kNmsStack / 2; ++k) stack[k] = stack[k + kNmsStack / 2];
+          sp = kNmsStack / 2;
+        }
+        stack[sp++] = pend;
+      }
+    }
+  }
+}
+
+// The same suppression for radii up to RM with the window's states fetched first:
+// each window row's bytes arrive as aligned 32-bit words, all rows' loads issued
+// before any is used, so a visit costs one round trip for the states plus one per
+// candidate neighbour's response, instead of one per window pixel.  The visit's
+// logic (scan order, the pending neighbour chosen, the guard) is k_nms's.
+template <int RM>
+__global__ void __launch_bounds__(256) k_nms_w(int W, int H, int rad, DetWs d) {
+  constexpr int NR = 2 * RM + 1;                      // window rows
+  constexpr int NW = (2 * RM + 1 + 3) / 4;            // aligned words of a row segment
+  const int n = d.counters[0];
+  volatile uint8_t* st = d.state;
+  const volatile uint32_t* stw = reinterpret_cast<const volatile uint32_t*>(d.state);
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+    const int root = d.listA[q];
+    int stack[kNmsStack];
+    int guard = 0;
+    while (st[root] == 1) {
+      int sp = 0;
+      stack[sp++] = root;
+      while (sp > 0) {
+        if (++guard > kNmsGuard) {
+          d.counters[1] = 1;
+          return;
+        }
+        const int t = stack[sp - 1];
+        if (st[t] != 1) { --sp; continue; }
+        const int x = t % W, y = t / W;
+        const int x0 = max(x - rad, 0), x1 = min(x + rad, W - 1);
+        const float r = d.resp[t];
+        uint32_t seg[NR][NW];                         // byte i of row a: pixel x0 + i
+#pragma unroll
+        for (int a = 0; a < NR; ++a) {
+          const int py = y - RM + a;
+          const bool ok = a >= RM - rad && a <= RM + rad && py >= 0 && py < H;
+          const size_t b0 = size_t(ok ? py : y) * W + x0;
+          const size_t w0 = b0 >> 2;
+          uint32_t w[NW + 1];
+#pragma unroll
+          for (int k = 0; k <= NW; ++k) w[k] = stw[w0 + k];
+          const uint32_t sel = 0x3210u + 0x1111u * uint32_t(b0 & 3);
+#pragma unroll
+          for (int k = 0; k < NW; ++k) seg[a][k] = ok ? __byte_perm(w[k], w[k + 1], sel) : 0u;
+        }
+        bool supp = false;
+        int pend = -1;
+#pragma unroll
+        for (int a = 0; a < NR; ++a) {
+          const int py = y - RM + a;
+#pragma unroll
+          for (int i = 0; i < 2 * RM + 1; ++i) {
+            if (supp || x0 + i > x1) continue;
+            const int s = int((seg[a][i >> 2] >> (8 * (i & 3))) & 0xFFu);
+            const int j = py * W + x0 + i;
+            if (s == 0 || s == 3 || j == t) continue;
+            if (!stronger(d.resp[j], j, r, t)) continue;
+            if (s == 2) supp = true;
+            else pend = j;
           }
         }
         if (supp) { st[t] = 3; --sp; continue; }
@@ -939,7 +1011,10 @@ int detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* c, de_ke
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  k_nms<<<sms * 8, 256, 0, s>>>(W, H, std::max(1, c->nms_radius), d);
+  const int rad = std::max(1, c->nms_radius);
+  if (rad <= 3) k_nms_w<3><<<sms * 8, 256, 0, s>>>(W, H, rad, d);
+  else if (rad <= 7) k_nms_w<7><<<sms * 8, 256, 0, s>>>(W, H, rad, d);
+  else k_nms<<<sms * 8, 256, 0, s>>>(W, H, rad, d);
   const int capk = ((cell + 1) / 2) * ((cell + 1) / 2);
   const size_t sm = size_t(capk) * (sizeof(de_keypoint) + sizeof(int));
   e = cudaFuncSetAttribute(k_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));

@@ -67,6 +67,9 @@ DET_CASES = [
     ("cell24", dict(cell=24)),
     ("dense_noref", dict(per_cell=6, subpixel=0)),
     ("nms1", dict(nms_radius=1, per_cell=8)),
+    ("nms5", dict(nms_radius=5, per_cell=8)),          # the word-fetch suppression up to 7
+    ("nms7", dict(nms_radius=7, per_cell=8)),
+    ("nms9", dict(nms_radius=9, per_cell=8)),          # the per-pixel suppression above 7
     ("grad5", dict(grad_window=5)),
     ("thr20", dict(fast_threshold=20, min_response=20.0)),
     ("cell128", dict(cell=128, per_cell=40)),

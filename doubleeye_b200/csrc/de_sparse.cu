@@ -551,6 +551,7 @@ struct MatchArgs {
   de_match_stats* stats;
   float max_dy, min_disp, max_disp, sigma_y, w_y, damping, lambda, gamma, eps;
   int maxc, iters, census_bits;
+  int smem_bytes;         // dynamic shared memory of the launch
 };
 
 __device__ __forceinline__ uint32_t ord_f32(float v) {   // order-preserving bits
@@ -730,6 +731,36 @@ __global__ void __launch_bounds__(1024, 1) k_match(MatchArgs a, MatchWs m) {
   __syncthreads();
 
   // --- damped max-sum sweeps ---------------------------------------------------------
+  // The sweeps walk each point's edges with dependent loads, so their state (row and
+  // column offsets, column items, scores, beta, rho) moves to shared memory when it
+  // fits (a few thousand edges take well under the 227 KB); the sort keys there are
+  // dead by now.  Same operations in the same order either way.
+  const int* bcnt = m.cnt;
+  const int* bcst = m.cstart;
+  const int* bcit = m.citems;
+  const float* bes = m.es;
+  float* bbeta = m.beta;
+  float* brho = m.rho;
+  const size_t bp_bytes = size_t(nl + 1 + nr + 1) * 4 + size_t(E) * 16;
+  const bool bp_smem = bp_bytes <= size_t(a.smem_bytes);
+  if (bp_smem) {
+    int* s_cnt = reinterpret_cast<int*>(smem);
+    int* s_cst = s_cnt + (nl + 1);
+    int* s_cit = s_cst + (nr + 1);
+    float* s_es = reinterpret_cast<float*>(s_cit + E);
+    float* s_beta = s_es + E;
+    float* s_rho = s_beta + E;
+    for (int i = tid; i <= nl; i += NT) s_cnt[i] = m.cnt[i];
+    for (int j = tid; j <= nr; j += NT) s_cst[j] = m.cstart[j];
+    for (int e = tid; e < E; e += NT) {
+      s_cit[e] = m.citems[e];
+      s_es[e] = m.es[e];
+      s_beta[e] = 0.f;
+      s_rho[e] = 0.f;
+    }
+    __syncthreads();
+    bcnt = s_cnt; bcst = s_cst; bcit = s_cit; bes = s_es; bbeta = s_beta; brho = s_rho;
+  }
   const float d0 = (a.damping < 0.f) ? 0.f : a.damping;
   const float dmp = (0.99f < d0) ? 0.99f : d0;
   float prev = 1e30f, md = 0.f;
@@ -737,40 +768,40 @@ __global__ void __launch_bounds__(1024, 1) k_match(MatchArgs a, MatchWs m) {
   for (; it < a.iters && E > 0; ++it) {
     float loc = 0.f;
     for (int i = tid; i < nl; i += NT) {
-      const int b = m.cnt[i], c = m.cnt[i + 1];
+      const int b = bcnt[i], c = bcnt[i + 1];
       float best = kNegBig, second = kNegBig;
       int bi = -1;
       for (int e = b; e < c; ++e) {
-        const float v = m.beta[e];
+        const float v = bbeta[e];
         if (v > best) { second = best; best = v; bi = e; } else if (v > second) second = v;
       }
       for (int e = b; e < c; ++e) {
         const float comp = fmax_ref(a.lambda, (e == bi) ? second : best);
-        const float tgt = m.es[e] - comp;
-        const float old = m.rho[e];
+        const float tgt = bes[e] - comp;
+        const float old = brho[e];
         const float upd = (1.f - dmp) * tgt + dmp * old;
         loc = fmax_ref(loc, fabsf(upd - old));
-        m.rho[e] = upd;
+        brho[e] = upd;
       }
     }
     __syncthreads();
     for (int j = tid; j < nr; j += NT) {
-      const int b = m.cstart[j], c = m.cstart[j + 1];
+      const int b = bcst[j], c = bcst[j + 1];
       float best = kNegBig, second = kNegBig;
       int bi = -1;
       for (int q = b; q < c; ++q) {
-        const int e = m.citems[q];
-        const float v = m.rho[e];
+        const int e = bcit[q];
+        const float v = brho[e];
         if (v > best) { second = best; best = v; bi = e; } else if (v > second) second = v;
       }
       for (int q = b; q < c; ++q) {
-        const int e = m.citems[q];
+        const int e = bcit[q];
         const float comp = fmax_ref(a.gamma, (e == bi) ? second : best);
-        const float tgt = m.es[e] - comp;
-        const float old = m.beta[e];
+        const float tgt = bes[e] - comp;
+        const float old = bbeta[e];
         const float upd = (1.f - dmp) * tgt + dmp * old;
         loc = fmax_ref(loc, fabsf(upd - old));
-        m.beta[e] = upd;
+        bbeta[e] = upd;
       }
     }
     md = cta_max(loc, redf);            // includes the barrier the next sweep needs
@@ -781,6 +812,14 @@ __global__ void __launch_bounds__(1024, 1) k_match(MatchArgs a, MatchWs m) {
       ++it;
       break;
     }
+  }
+
+  if (bp_smem) {                      // the later stages read beta and rho globally
+    for (int e = tid; e < E; e += NT) {
+      m.beta[e] = bbeta[e];
+      m.rho[e] = brho[e];
+    }
+    __syncthreads();
   }
 
   // --- belief, margins, mutual best ----------------------------------------------------
@@ -1095,9 +1134,18 @@ int match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl, const int
   MatchWs m = carve_match(ws, std::max(nl, 1), std::max(nr, 1), maxc);
   int N = 1;
   while (N < std::max(nr, 1)) N <<= 1;
-  const size_t sm = std::max(size_t(N) * 8, size_t(1024));
-  cudaError_t e = cudaFuncSetAttribute(k_match, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(sm));
+  // the sort keys need N * 8 bytes; the BP sweeps use whatever the SM offers beyond
+  // (one CTA per problem, so the whole of it)
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, k_match);
+  if (e != cudaSuccess) return set_error(DE_ERR_CUDA, "k_match attributes: %s", cudaGetErrorString(e));
+  const size_t avail = size_t(std::max(0, optin - int(fa.sharedSizeBytes))) & ~size_t(15);
+  const size_t sm = std::max(std::max(size_t(N) * 8, size_t(1024)), avail);
+  a.smem_bytes = int(sm);
+  e = cudaFuncSetAttribute(k_match, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
   if (e != cudaSuccess) return set_error(DE_ERR_CUDA, "k_match smem: %s", cudaGetErrorString(e));
   k_match<<<1, 1024, sm, s>>>(a, m);
   e = cudaGetLastError();

@@ -39,7 +39,7 @@ def disp_evals(n_pairs: int) -> float:
     return float(n_pairs) * W * H * D
 
 
-# Algorithmic bytes per pair and per stage ("Roofline"): compulsory
+# Algorithmic bytes per pair and per stage: compulsory
 # traffic of each kernel if every operand is touched once.
 WH = W * H
 E = WH * D
@@ -72,13 +72,13 @@ def measure_int_rates(device: int) -> dict:
     """Lane operations per SM clock of each probed op (de_int_probe), timed with
     CUDA events; the SM clock is sampled around the probe."""
     import torch
-    from doubleeye_b200._lib import lib
+    from doubleeye_b200._lib import probe_lib
     sms = torch.cuda.get_device_properties(device).multi_processor_count
     out = {}
     with ClockSampler(device) as clk:
         for name, op in PROBE_OPS.items():
             ms, n = C.c_float(), C.c_double()
-            if lib().de_int_probe(op, 1000 if name == "popc" else 3000, None,
+            if probe_lib().de_int_probe(op, 1000 if name == "popc" else 3000, None,
                                   C.byref(ms), C.byref(n)) != 0:
                 return {}
             out[name] = n.value / (ms.value * 1e-3) / sms

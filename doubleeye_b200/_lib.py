@@ -99,8 +99,6 @@ SIGNATURES = {
     "de_set_param": (C.c_int, [C.c_char_p, C.c_int]),
     "de_get_param": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
     "de_stage_times": (C.c_int, [C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_int)]),
-    "de_int_probe": (C.c_int, [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_float),
-                              C.POINTER(C.c_double)]),
     "de_ctx_create": (C.c_int, [C.POINTER(DeCfg), C.c_int, C.POINTER(vp)]),
     "de_ctx_destroy": (C.c_int, [vp]),
     "de_ctx_set_cfg": (C.c_int, [vp, C.POINTER(DeCfg)]),
@@ -202,6 +200,27 @@ def get_param(name: str) -> int:
     v = C.c_int()
     check(lib().de_get_param(name.encode(), C.byref(v)))
     return v.value
+
+
+PROBE_PATH = os.path.join(PKG, "_lib", "libde_probe.so")
+_probe = None
+
+
+def probe_lib() -> C.CDLL:
+    """The bench's integer-pipe probe (de_int_probe), a library of its own outside the
+    matcher's C ABI: (op, trips, stream, float* ms, double* lane_ops) -> status."""
+    global _probe
+    with _lock:
+        if _probe is None:
+            if not os.path.exists(PROBE_PATH):
+                raise RuntimeError(f"{PROBE_PATH} is missing: build with "
+                                   "`python -m doubleeye_b200.build`")
+            L = C.CDLL(PROBE_PATH)
+            L.de_int_probe.restype = C.c_int
+            L.de_int_probe.argtypes = [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_float),
+                                       C.POINTER(C.c_double)]
+            _probe = L
+    return _probe
 
 
 def exported_symbols() -> list[str]:

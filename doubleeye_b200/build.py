@@ -18,7 +18,10 @@ OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdoubleeye_b200.so")
 
 SOURCES = ["de_dense.cu", "de_capi.cu", "de_noalloc.cu", "de_sparse.cu", "de_edges.cu",
-           "de_serve.cu", "de_graph.cu", "de_prior.cu", "de_probe.cu"]
+           "de_serve.cu", "de_graph.cu", "de_prior.cu"]
+# the bench's integer-pipe probe: its own library, outside the matcher's C ABI
+PROBE_SRC = "de_probe.cu"
+PROBE_LIB = os.path.join(OUT_DIR, "libde_probe.so")
 TOOLS = os.path.join(PKG, "tools")
 CLI = os.path.join(OUT_DIR, "de_dense_gpu")      # the reference-compatible command line
 NVCC_FLAGS = [
@@ -54,7 +57,7 @@ def stale() -> bool:
     if not os.path.exists(stamp) or open(stamp).read() != _stamp():
         return True
     t = os.path.getmtime(LIB)
-    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
+    deps = sources() + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f != PROBE_SRC]
     deps.append(os.path.join(os.path.dirname(PKG), "include", "doubleeye_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
@@ -77,7 +80,22 @@ def build_cli(force: bool = False, verbose: bool = False) -> str:
     return CLI
 
 
+def build_probe(force: bool = False, verbose: bool = False) -> str:
+    src = os.path.join(CSRC, PROBE_SRC)
+    if not force and os.path.exists(PROBE_LIB) and \
+            os.path.getmtime(PROBE_LIB) >= os.path.getmtime(src):
+        return PROBE_LIB
+    os.makedirs(OUT_DIR, exist_ok=True)
+    cmd = [nvcc()] + NVCC_FLAGS + ["-o", PROBE_LIB + ".tmp", src]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(PROBE_LIB + ".tmp", PROBE_LIB)
+    return PROBE_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    build_probe(force, verbose)
     if not force and not stale():
         build_cli(False, verbose)
         return LIB

@@ -557,7 +557,12 @@ int de_get_param(const char* name, int* value) {
 }
 
 int de_workspace_status(const void* workspace, void* stream, int* status) {
-  if (!workspace || !status) return fail(DE_ERR_ARG, "NULL argument");
+  if (!status) return fail(DE_ERR_ARG, "NULL argument");
+  if (!workspace) {                    // the no-allocation entry point's scratch
+    void* head = nullptr;
+    if (const int rc = de::noalloc_status_word(&head)) return rc;
+    workspace = head;
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   DE_CUDA(cudaMemcpyAsync(status, workspace, sizeof(int), cudaMemcpyDeviceToHost, s));
   DE_CUDA(cudaStreamSynchronize(s));

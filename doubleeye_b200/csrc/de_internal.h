@@ -73,6 +73,10 @@ struct Batch {
   DevPair p[kMaxBatch];
 };
 
+// Device address of the no-allocation entry point's status word on the current device
+// (de_noalloc.cu); DE_OK or an error code already recorded for de_last_error().
+int noalloc_status_word(void** out);
+
 // Records a one-line reason for de_last_error() and returns code (de_capi.cu).
 int set_error(int code, const char* fmt, ...);
 

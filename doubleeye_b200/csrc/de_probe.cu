@@ -1,5 +1,14 @@
 // Integer-pipe throughput probe: the denominators of the INT roofline the dense
-// kernels are reported against.  No counterpart in the reference.
+// kernels are reported against.  No counterpart in the reference.  It is a bench
+// instrument, built into its own library (_lib/libde_probe.so), not part of the
+// matcher's C ABI:
+//
+//   int de_int_probe(int op, int trips, void* stream, float* ms, double* lane_ops)
+//
+// runs op 0 add.u32, 1 lop3.b32, 2 shf (funnel rotate), 3 mad.lo.u32 or 4 popc.b32 as
+// 8 independent chains per thread on every SM for `trips` loop trips; *ms is the
+// CUDA-event time of the timed launch and *lane_ops the warp-lane operations it
+// executed, so lane_ops / (ms * SM clock * SMs) is the op's rate per SM clock.
 //
 // Each thread runs 8 independent accumulator chains of one instruction class, 16 x 8
 // instructions per loop trip, written as inline PTX so the chains are neither folded
@@ -11,7 +20,7 @@
 
 #include <cstdint>
 
-#include "de_internal.h"
+#include "../../include/doubleeye_b200.h"
 
 namespace {
 
@@ -52,7 +61,7 @@ __global__ void __launch_bounds__(256) k_int_probe(uint32_t* sink, int trips, ui
 
 }  // namespace
 
-extern "C" int de_int_probe(int op, int trips, void* stream, float* ms, double* lane_ops) {
+extern "C" __attribute__((visibility("default"))) int de_int_probe(int op, int trips, void* stream, float* ms, double* lane_ops) {
   if (op < 0 || op > 4 || trips < 1 || !ms || !lane_ops) return DE_ERR_ARG;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int dev = 0, nsm = 0;

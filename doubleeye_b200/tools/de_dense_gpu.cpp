@@ -22,7 +22,6 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <map>
 #include <string>
 #include <vector>
 
@@ -56,6 +55,209 @@ bool dump(const std::string& p, const float* v, size_t n) {
 bool read_all(void* p, size_t n) { return std::fread(p, 1, n, stdin) == n; }
 
 bool write_all(const void* p, size_t n) { return std::fwrite(p, 1, n, stdout) == n; }
+
+// ---- --prior ------------------------------------------------------------------
+// The prior file holds float32 disparities, either one per pixel (W*H) or one per
+// 2x2 block (floor(W/2) * floor(H/2)), the latter read as nearest-neighbour samples
+// at twice the disparity.  A non-finite value is a hole, and a prior with holes is
+// refused.  Interface: core/tools/de_dense.cpp --prior (flag at :1756).
+bool slurp(const std::string& path, std::vector<unsigned char>* bytes) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) return false;
+  unsigned char chunk[1 << 16];
+  size_t n;
+  while ((n = std::fread(chunk, 1, sizeof(chunk), f)) > 0) bytes->insert(bytes->end(), chunk, chunk + n);
+  const bool ok = !std::ferror(f);
+  std::fclose(f);
+  return ok;
+}
+
+bool load_prior(const std::string& path, int W, int H, std::vector<float>* prior,
+                std::string* why) {
+  std::vector<unsigned char> raw;
+  if (!slurp(path, &raw)) {
+    *why = "not readable";
+    return false;
+  }
+  const size_t full = size_t(W) * H;
+  const int hw = W / 2, hh = H / 2;
+  const size_t half = size_t(hw) * hh;
+  const size_t count = raw.size() / sizeof(float);
+  if (raw.size() % sizeof(float) != 0 || (count != full && count != half)) {
+    *why = std::to_string(raw.size()) + " bytes; want " + std::to_string(full * 4) +
+           " (" + std::to_string(W) + "x" + std::to_string(H) + " float32) or " +
+           std::to_string(half * 4) + " (" + std::to_string(hw) + "x" + std::to_string(hh) +
+           ", half resolution)";
+    return false;
+  }
+  std::vector<float> src(count);
+  std::memcpy(src.data(), raw.data(), count * sizeof(float));
+  prior->assign(full, 0.f);
+  if (count == full) {
+    *prior = std::move(src);
+  } else {
+    // each full-resolution pixel samples the block it falls in (the last block row /
+    // column also covers an odd trailing pixel), disparity scaled to full resolution
+    for (int y = 0; y < H; ++y) {
+      const float* srow = src.data() + size_t(y / 2 < hh ? y / 2 : hh - 1) * hw;
+      float* drow = prior->data() + size_t(y) * W;
+      for (int x = 0; x < W; ++x) drow[x] = 2.f * srow[x / 2 < hw ? x / 2 : hw - 1];
+    }
+  }
+  const size_t bad = size_t(std::count_if(prior->begin(), prior->end(),
+                                          [](float v) { return !std::isfinite(v); }));
+  if (bad) {
+    *why = std::to_string(bad) + " of " + std::to_string(full) +
+           " values are holes (non-finite); fill them before matching";
+    return false;
+  }
+  return true;
+}
+
+// ---- --stream -----------------------------------------------------------------
+// Wire format (interface of core/tools/de_dense_cuda.cu:44-59):
+//   in   "DEIR" | width u16 | height u16 | camera u8 | flags u8 | frame u32 | Y8 image
+//   out  "DEDD" | width u16 | height u16 | frame u32 | flags u32 | left Y8 |
+//        W*H int16 disparity in 1/16 px (-32768 = declined) | W*H u8 confidence if
+//        flags & 1
+// Camera 1 is the left image.  Two images with the same frame number from the two
+// cameras make a pair; a later image from the same camera replaces the earlier one.
+// At most kWaiting frames wait for their partner; when a ninth arrives, the lowest
+// frame number of the nine is given up.
+constexpr int kWaiting = 8;
+
+struct FrameSlot {
+  bool used = false;
+  uint32_t frame = 0;
+  bool has[2] = {false, false};   // [0] right camera, [1] left camera
+  std::vector<uint8_t> img[2];
+};
+
+class FramePairer {
+ public:
+  explicit FramePairer(size_t bytes) : bytes_(bytes) {
+    for (FrameSlot& s : slots_) { s.img[0].resize(bytes); s.img[1].resize(bytes); }
+  }
+  // Stores the image that was read into scratch(); returns the slot if that
+  // completed a pair, else nullptr.
+  FrameSlot* offer(uint32_t frame, int camera) {
+    const int side = camera == 1 ? 1 : 0;
+    FrameSlot* s = find(frame);
+    if (!s) s = claim(frame);
+    if (!s) { ++discarded_; return nullptr; }   // older than every waiting frame
+    std::swap(s->img[side], scratch_);
+    if (scratch_.size() != bytes_) scratch_.resize(bytes_);
+    s->has[side] = true;
+    return (s->has[0] && s->has[1]) ? s : nullptr;
+  }
+  void release(FrameSlot* s) { s->used = false; s->has[0] = s->has[1] = false; }
+  uint8_t* scratch() { if (scratch_.size() != bytes_) scratch_.resize(bytes_); return scratch_.data(); }
+  long discarded() const { return discarded_; }
+
+ private:
+  FrameSlot* find(uint32_t frame) {
+    for (FrameSlot& s : slots_) if (s.used && s.frame == frame) return &s;
+    return nullptr;
+  }
+  // A free slot, else the slot of the lowest waiting frame number, which is given up;
+  // nullptr when the new frame itself is the lowest (it is the one given up).
+  FrameSlot* claim(uint32_t frame) {
+    FrameSlot* victim = nullptr;
+    for (FrameSlot& s : slots_) {
+      if (!s.used) { victim = &s; break; }
+      if (!victim || s.frame < victim->frame) victim = &s;
+    }
+    if (victim->used && frame < victim->frame) return nullptr;
+    if (victim->used) ++discarded_;
+    release(victim);
+    victim->used = true;
+    victim->frame = frame;
+    return victim;
+  }
+  size_t bytes_;
+  FrameSlot slots_[kWaiting];
+  std::vector<uint8_t> scratch_;
+  long discarded_ = 0;
+};
+
+template <typename T>
+T get_le(const unsigned char* p) {
+  T v;
+  std::memcpy(&v, p, sizeof(T));
+  return v;
+}
+template <typename T>
+void put_le(unsigned char* p, T v) { std::memcpy(p, &v, sizeof(T)); }
+
+// Sixteenths of a pixel, round half up; -32768 (and confidence 0) where the matcher
+// gave no positive, finite disparity.
+void encode_q4(const std::vector<float>& disp, std::vector<int16_t>* q4,
+               std::vector<uint8_t>* conf) {
+  for (size_t i = 0; i < disp.size(); ++i) {
+    const float d = disp[i];
+    const bool ok = std::isfinite(d) && d > 0.f;
+    (*q4)[i] = ok ? int16_t(std::floor(double(d) * 16.0 + 0.5)) : int16_t(-32768);
+    if (!ok && conf) (*conf)[i] = 0;
+  }
+}
+
+int serve_stream(de_ctx* ctx, int W, int H, bool want_conf) {
+  const size_t WH = size_t(W) * H;
+  FramePairer pairer(WH);
+  std::vector<float> disp(WH);
+  std::vector<int16_t> q4(WH);
+  std::vector<uint8_t> conf(WH);
+  long served = 0;
+  double last_note = now_ms();
+  unsigned char in[14];
+  while (read_all(in, sizeof(in))) {
+    if (std::memcmp(in, "DEIR", 4) != 0) {
+      std::fprintf(stderr, "de_dense_gpu: input is not a DEIR frame header; giving up\n");
+      return 1;
+    }
+    const int fw = get_le<uint16_t>(in + 4), fh = get_le<uint16_t>(in + 6);
+    const int camera = in[8];
+    const uint32_t frame = get_le<uint32_t>(in + 10);
+    if (fw != W || fh != H) {
+      std::fprintf(stderr, "de_dense_gpu: frame %u is %dx%d; the matcher runs at %dx%d\n",
+                   frame, fw, fh, W, H);
+      return 1;
+    }
+    if (!read_all(pairer.scratch(), WH)) break;          // truncated image: end of input
+    FrameSlot* pair = pairer.offer(frame, camera);
+    if (!pair) continue;
+    const uint8_t* left = pair->img[1].data();
+    const uint8_t* right = pair->img[0].data();
+    if (de_ctx_dense(ctx, left, right, W, H, disp.data(), nullptr,
+                     want_conf ? conf.data() : nullptr, nullptr) != DE_OK) {
+      std::fprintf(stderr, "de_dense_gpu: frame %u: %s\n", frame, de_last_error());
+      return 1;
+    }
+    encode_q4(disp, &q4, want_conf ? &conf : nullptr);
+    unsigned char out[16];
+    std::memcpy(out, "DEDD", 4);
+    put_le<uint16_t>(out + 4, uint16_t(W));
+    put_le<uint16_t>(out + 6, uint16_t(H));
+    put_le<uint32_t>(out + 8, frame);
+    put_le<uint32_t>(out + 12, want_conf ? 1u : 0u);
+    const bool wrote = write_all(out, sizeof(out)) && write_all(left, WH) &&
+                       write_all(q4.data(), WH * sizeof(int16_t)) &&
+                       (!want_conf || write_all(conf.data(), WH));
+    pairer.release(pair);
+    if (!wrote) break;                                   // reader went away
+    std::fflush(stdout);
+    ++served;
+    const double t = now_ms();
+    if (t - last_note > 5000.0) {
+      std::fprintf(stderr, "de_dense_gpu: served %ld frame pairs (%ld images had no partner)\n",
+                   served, pairer.discarded());
+      last_note = t;
+    }
+  }
+  std::fprintf(stderr, "de_dense_gpu: end of input after %ld frame pairs (%ld images had no "
+                       "partner)\n", served, pairer.discarded());
+  return 0;
+}
 
 int usage(const char* argv0) {
   std::fprintf(stderr,
@@ -130,76 +332,9 @@ int main(int argc, char** argv) {
   std::vector<uint8_t> conf(WH);
 
   if (stream_mode) {
-    struct Pending { std::vector<uint8_t> img; int stream; };
-    std::map<uint32_t, Pending> pending;
-    std::vector<int16_t> q(WH);
-    long pairs = 0, dropped = 0;
-    for (;;) {
-      unsigned char hdr[14];
-      if (!read_all(hdr, sizeof(hdr))) break;
-      if (std::memcmp(hdr, "DEIR", 4) != 0) {
-        std::fprintf(stderr, "de_dense_gpu: lost sync (bad magic), stopping\n");
-        de_ctx_destroy(ctx);
-        return 1;
-      }
-      uint16_t pw, ph;
-      uint32_t num;
-      std::memcpy(&pw, hdr + 4, 2);
-      std::memcpy(&ph, hdr + 6, 2);
-      const int st = hdr[8];
-      std::memcpy(&num, hdr + 10, 4);
-      if (int(pw) != W || int(ph) != H) {
-        std::fprintf(stderr, "de_dense_gpu: stream is %dx%d, this was started for %dx%d\n",
-                     int(pw), int(ph), W, H);
-        de_ctx_destroy(ctx);
-        return 1;
-      }
-      std::vector<uint8_t> img(WH);
-      if (!read_all(img.data(), WH)) break;
-      auto it = pending.find(num);
-      if (it == pending.end()) {
-        pending[num] = Pending{std::move(img), st};
-        while (pending.size() > 8) { pending.erase(pending.begin()); ++dropped; }
-        continue;
-      }
-      if (it->second.stream == st) { it->second.img = std::move(img); continue; }
-      const std::vector<uint8_t>& lft = (st == 1) ? img : it->second.img;
-      const std::vector<uint8_t>& rgt = (st == 1) ? it->second.img : img;
-      if (de_ctx_dense(ctx, lft.data(), rgt.data(), W, H, disp.data(), nullptr,
-                       want_conf ? conf.data() : nullptr, nullptr) != DE_OK) {
-        std::fprintf(stderr, "de_dense_gpu: %s\n", de_last_error());
-        de_ctx_destroy(ctx);
-        return 1;
-      }
-      for (size_t i = 0; i < WH; ++i) {
-        const float d = disp[i];
-        q[i] = (d > 0.f && std::isfinite(d)) ? int16_t(std::lround(d * 16.0f))
-                                               : int16_t(-32768);
-        if (want_conf && q[i] == int16_t(-32768)) conf[i] = 0;
-      }
-      unsigned char out[16];
-      std::memcpy(out, "DEDD", 4);
-      std::memcpy(out + 4, &pw, 2);
-      std::memcpy(out + 6, &ph, 2);
-      std::memcpy(out + 8, &num, 4);
-      const uint32_t flags = want_conf ? 1u : 0u;
-      std::memcpy(out + 12, &flags, 4);
-      if (!write_all(out, sizeof(out)) || !write_all(lft.data(), WH) ||
-          !write_all(q.data(), WH * sizeof(int16_t)) ||
-          (want_conf && !write_all(conf.data(), WH)))
-        break;
-      std::fflush(stdout);
-      pending.erase(it);
-      if (++pairs % 30 == 0) {
-        size_t filled = 0;
-        for (size_t i = 0; i < WH; ++i) filled += q[i] != int16_t(-32768);
-        std::fprintf(stderr, "de_dense_gpu: %ld pairs, %ld unpaired dropped, %.0f%% filled\n",
-                     pairs, dropped, 100.0 * double(filled) / double(WH));
-      }
-    }
-    std::fprintf(stderr, "de_dense_gpu: %ld pairs, %ld unpaired dropped\n", pairs, dropped);
+    const int rc = serve_stream(ctx, W, H, want_conf);
     de_ctx_destroy(ctx);
-    return 0;
+    return rc;
   }
 
   std::vector<uint8_t> L, R;
@@ -208,48 +343,17 @@ int main(int argc, char** argv) {
     de_ctx_destroy(ctx);
     return 1;
   }
-  // --prior F: W*H floats, or (W/2)*(H/2) upsampled by nearest neighbour with the
-  // disparity doubled; holes are refused (core/tools/de_dense.cpp:1756-1813)
   std::vector<float> prior;
   if (!priorp.empty()) {
-    FILE* f = std::fopen(priorp.c_str(), "rb");
-    if (!f) {
-      std::fprintf(stderr, "cannot open prior %s\n", priorp.c_str());
-      de_ctx_destroy(ctx);
-      return 1;
-    }
-    std::fseek(f, 0, SEEK_END);
-    const size_t n = size_t(std::ftell(f)) / sizeof(float);
-    std::fseek(f, 0, SEEK_SET);
-    std::vector<float> raw(n);
-    const size_t got = std::fread(raw.data(), sizeof(float), n, f);
-    std::fclose(f);
-    const int W2 = W / 2, H2 = H / 2;
-    if (got != n || (n != WH && n != size_t(W2) * H2)) {
-      std::fprintf(stderr, "prior %s has %zu floats, expected %zu (full) or %zu (half)\n",
-                   priorp.c_str(), n, WH, size_t(W2) * H2);
-      de_ctx_destroy(ctx);
-      return 1;
-    }
-    prior.resize(WH);
-    if (n == WH) {
-      prior = raw;
-    } else {
-      for (int y = 0; y < H; ++y)
-        for (int x = 0; x < W; ++x)
-          prior[size_t(y) * W + x] =
-              2.f * raw[size_t(std::min(H2 - 1, y / 2)) * W2 + std::min(W2 - 1, x / 2)];
-    }
-    size_t holes = 0;
-    for (float v : prior) holes += std::isfinite(v) ? 0 : 1;
-    if (holes) {
-      std::fprintf(stderr, "prior has %zu holes of %zu; fill them first\n", holes, WH);
+    std::string why;
+    if (!load_prior(priorp, W, H, &prior, &why)) {
+      std::fprintf(stderr, "de_dense_gpu: --prior %s: %s\n", priorp.c_str(), why.c_str());
       de_ctx_destroy(ctx);
       return 1;
     }
     if (cfg.subpixel)
-      std::fprintf(stderr, "note: --prior disables sub-pixel (masked planes break the "
-                           "neighbour invariant); disparities are integer\n");
+      std::fprintf(stderr, "de_dense_gpu: --prior runs without sub-pixel refinement "
+                           "(disparities are whole pixels)\n");
   }
   std::vector<float> cand(confp.empty() ? 0 : WH * 6);
   de_stage_timing(1);

@@ -111,20 +111,24 @@ DE_API int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n,
                         void* workspace, size_t ws_bytes, void* stream);
 
 /* The same dense pipeline for one pair with NO allocation anywhere: for callers
- * that cannot call cudaMalloc (inside a graph capture that must not allocate, on
- * real-time threads, under a host that owns the device heap).  No counterpart in
- * the reference.  The workspace is a 16 MiB file-scope device array that every GPU
- * loading this library holds until exit; a pair whose de_dense_workspace_bytes
- * exceeds it is refused with DE_ERR_ARG (the default 7x7 census fits 320x240 at
- * D <= 64).  The first call on a device resolves the array's device address with
- * that device current, so make that first call before any stream capture.  Calls
- * share the array: calls whose work overlaps on the GPU (concurrent streams,
- * devices aside) race and must be serialised by the caller. */
+ * that cannot call cudaMalloc (real-time threads that may not take the driver's
+ * allocation locks, hosts that own the device heap, integrations whose memory budget
+ * is fixed up front).  No counterpart in the reference.  The workspace is a 16 MiB
+ * file-scope device array that every GPU loading this library holds until exit; a
+ * pair whose de_dense_workspace_bytes exceeds it is refused with DE_ERR_ARG (the
+ * default 7x7 census fits 320x240 at D <= 64).  The first call on a device resolves
+ * the array's device address with that device current and keeps it, so a device
+ * reset while the library is loaded is not supported.  Calls share the array and
+ * each leaves its contents behind: calls whose work overlaps on the GPU (concurrent
+ * streams) race and must be serialised by the caller.  The status of the last call
+ * is read with de_workspace_status(NULL, stream, &status). */
 DE_API int de_dense_noalloc_dev(const de_cfg* cfg, const de_pair* pair, void* stream);
 
 /* Status of the last launch set that used this workspace: waits for the stream,
  * then writes 0, or non-zero if a bounded device wait ran out (the results of that
- * launch set are then invalid).  The host-pointer context checks it itself. */
+ * launch set are then invalid).  The host-pointer context checks it itself.
+ * workspace NULL reads the status of the last de_dense_noalloc_dev call on the
+ * current device. */
 DE_API int de_workspace_status(const void* workspace, void* stream, int* status);
 
 /* Stage entry points, for stage-level parity and for callers that keep their
@@ -155,14 +159,6 @@ DE_API int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const 
  * sets into *launches, and clears them. */
 DE_API int de_stage_timing(int enable);
 DE_API int de_stage_times(float* ms, int n, int* launches);
-
-/* Integer-pipe throughput probe (no counterpart in the reference): runs op 0 add.u32,
- * 1 lop3.b32, 2 shf (funnel rotate), 3 mad.lo.u32 or 4 popc.b32 as 8 independent
- * chains per thread on every SM for `trips` loop trips; *ms is the CUDA-event time
- * of the timed launch and *lane_ops the warp-lane operations it executed, so
- * lane_ops / (ms * SM clock * SMs) is the op's rate per SM clock.  The denominators
- * of the dense kernels' integer roofline. */
-DE_API int de_int_probe(int op, int trips, void* stream, float* ms, double* lane_ops);
 
 /* Launch-shape knobs (process-wide; results never depend on them, only speed).
  * No counterpart in the reference, whose launch shapes are fixed.

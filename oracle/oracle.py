@@ -107,6 +107,17 @@ P_U8, P_U16, P_I16, P_I32, P_U64, P_F32 = (C.c_uint8, C.c_uint16, C.c_int16, C.c
                                            C.c_uint64, C.c_float)
 
 
+def reference_root() -> str:
+    """The reference project's root (the directory holding core/ and article/), from
+    the DOUBLEEYE_REF environment variable; only the fixture generators and the
+    reference build read the reference tree, and they need it named explicitly."""
+    root = os.environ.get("DOUBLEEYE_REF", "")
+    if not root or not os.path.isdir(os.path.join(root, "core")):
+        raise RuntimeError("set DOUBLEEYE_REF to the reference project's root "
+                           "(the directory holding core/ and article/)")
+    return root
+
+
 def build(ref: bool = False) -> None:
     """Build liboracle.so (and _ref/ when asked and the reference tree exists)."""
     targets = ["oracle"] + (["ref"] if ref else [])

@@ -21,7 +21,7 @@ sys.path.insert(0, REPO)
 from oracle import oracle as O  # noqa: E402
 from doubleeye_b200 import synth  # noqa: E402
 
-SCENES = "/root/reference/article/scenes"
+SCENES = os.path.join(O.reference_root(), "article", "scenes")
 
 # (name, W, H, cfg overrides) -- small enough for the single-threaded oracle to check
 # in well under a second each, spread over the configuration space the path supports.

@@ -25,7 +25,7 @@ sys.path.insert(0, REPO)
 from oracle import oracle as O  # noqa: E402
 from doubleeye_b200 import synth  # noqa: E402
 
-ARTICLE = "/root/reference/article"
+ARTICLE = os.path.join(O.reference_root(), "article")
 SCENES = os.path.join(ARTICLE, "scenes")
 
 

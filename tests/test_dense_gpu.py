@@ -207,7 +207,7 @@ def test_int_probe_rates():
     integer-capable pipes), with POPC on its slower pipe."""
     import ctypes as C
     import torch
-    from doubleeye_b200._lib import lib
+    from doubleeye_b200._lib import probe_lib as lib
     sms = torch.cuda.get_device_properties(0).multi_processor_count
     max_hz = 2.2e9                                     # above any B200 boost clock
     for op in range(5):

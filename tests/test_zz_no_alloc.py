@@ -1,13 +1,15 @@
 """The dense entry point that allocates nothing, de_dense_noalloc_dev.
 
-It exists for callers that cannot call cudaMalloc: work recorded inside a CUDA-graph
-capture that must not allocate, real-time threads that may not take the driver's
-allocation locks, and hosts that own the device heap.  Its scratch is a fixed
+It exists for callers that cannot call cudaMalloc: real-time threads that may not
+take the driver's allocation locks, hosts that own the device heap, and integrations
+whose memory budget is fixed before the process starts.  Its scratch is a fixed
 16 MiB device array built into the library, so it takes only the caller's images and
-output buffers.  These tests call it through the C ABI, twice in a row on one pair,
-and require each call to give the same bytes as the workspace entry point
-de_dense_dev (the dense path is bit-exact, so the tolerance is zero), and that a pair
-too large for the array is refused without running anything.
+output buffers.  These tests call it through the C ABI, twice in a row on one pair
+(with and without the reverse-match plane, which is carved from the same array), and
+require each call to give the same bytes as the workspace entry point de_dense_dev
+(the dense path is bit-exact, so the tolerance is zero), the device's free memory to
+be the same before and after a call, the status word to read 0, and a pair too large
+for the array to be refused without running anything.
 
 Kept in a file of its own, collected last, so a failure here leaves every other test
 already run; it also passes alone in a fresh process.
@@ -52,11 +54,12 @@ def _same(a, b):
     return bool((a == b).all())
 
 
-def test_noalloc_matches_workspace_entry_point(lib):
+@pytest.mark.parametrize("lrc", [0, 1])
+def test_noalloc_matches_workspace_entry_point(lib, lrc):
     import doubleeye_b200 as de
     from doubleeye_b200 import synth
     p = synth.slanted_planes(320, 240, 63, tag="noalloc")
-    cfg = de.Cfg(dmax=64, iters=8)
+    cfg = de.Cfg(dmax=64, iters=8, lrc=lrc)
     L = torch.from_numpy(p.left).cuda()
     R = torch.from_numpy(p.right).cuda()
     stream = torch.cuda.current_stream().cuda_stream
@@ -71,13 +74,22 @@ def test_noalloc_matches_workspace_entry_point(lib):
                                      stream))
     torch.cuda.synchronize()
 
+    outs = [_outputs(240, 320) for _ in range(2)]
+    pairs = [_pair(lib, L, R, o) for o in outs]
+    torch.cuda.synchronize()
     for call in range(2):                      # the scratch keeps the last call's contents
-        out = _outputs(240, 320)
-        lib.check(lib.lib().de_dense_noalloc_dev(C.byref(cfg), C.byref(_pair(lib, L, R, out)),
-                                                 stream))
+        free0 = torch.cuda.mem_get_info()[0]
+        held0 = torch.cuda.memory_allocated()
+        lib.check(lib.lib().de_dense_noalloc_dev(C.byref(cfg), C.byref(pairs[call]), stream))
         torch.cuda.synchronize()
+        if call == 1:                          # after the first call loaded every kernel
+            assert torch.cuda.mem_get_info()[0] == free0, "device free memory changed"
+        assert torch.cuda.memory_allocated() == held0
+        st = C.c_int(-1)
+        lib.check(lib.lib().de_workspace_status(None, stream, C.byref(st)))
+        assert st.value == 0
         for k in ("disp", "margin", "conf", "cand"):
-            assert _same(out[k], ref[k]), f"call {call}: {k} differs from de_dense_dev"
+            assert _same(outs[call][k], ref[k]), f"call {call}: {k} differs from de_dense_dev"
     assert torch.isfinite(ref["disp"]).float().mean().item() > 0.5
 
 

@@ -57,6 +57,14 @@ void or_cost_top2_prior(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, i
 void or_dense_prior(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
                     const float* prior, int band, float* disp, float* margin, float* cand6);
 float or_confidence(float s1, float s2, float lambda, float lrc, float lrc_tol);
+
+/* double precision (de_oracle_f64.c), for the error statement against exact arithmetic */
+void or_cost_top2_f64(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                      double* cs, int* cd, int* cn, double* nb);
+void or_solve_row_f64(const de_cfg* cfg, int W, const double* cs, const int* cd,
+                      const int* cn, const double* nb, double* disp, double* best_out);
+void or_dense_f64(const de_cfg* cfg, const uint8_t* L, const uint8_t* R, int W, int H,
+                  double* disp, double* best);
 unsigned or_confidence_u8(float s1, float s2, float lambda, float lrc, float lrc_tol);
 
 /* sparse path (de_oracle_sparse.c) */

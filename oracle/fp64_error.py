@@ -14,6 +14,18 @@ reference's float rf_filter, :510-527), per configuration:
   * the fraction of pixels whose winning disparity (first maximum over planes in
     ascending order, as the top-2 insert keeps it) is the same under both.
 
+and how far the single-precision row solve (damped max-sum, belief, claim and
+sub-pixel fit: core/include/doubleeye/dense_solve.hpp:213-434) is from the same solve
+in double precision (or_solve_row_f64):
+
+  * solve only: the float solve and the double solve on the same candidates; the
+    fraction of pixels with the same answer (both declined, or disparities within
+    0.01 px), the largest disparity difference among them, and the largest belief
+    difference;
+  * end to end: the int16 filter + float solve (what the GPU computes, bit for bit)
+    against the double filter + double solve (exact arithmetic throughout); the
+    fraction of pixels with the same answer within 0.5 px and within 1 px.
+
     python -m oracle.fp64_error            # one JSON line per workload
 """
 from __future__ import annotations
@@ -72,6 +84,46 @@ def statement(orc: "O.Oracle", cfg: "O.DeCfg", L: np.ndarray, R: np.ndarray) -> 
             "winner_agreement": float((k_i[valid] == k_f[valid]).mean()), "values": n}
 
 
+NONE = -1e300
+
+
+def _same_answer(a: np.ndarray, b: np.ndarray, tol: float) -> np.ndarray:
+    fa, fb = np.isfinite(a), np.isfinite(b)
+    close = np.zeros(a.shape, bool)
+    both = fa & fb
+    close[both] = np.abs(a[both].astype(np.float64) - b[both]) <= tol
+    return (~fa & ~fb) | close
+
+
+def solve_statement(orc: "O.Oracle", cfg: "O.DeCfg", L: np.ndarray, R: np.ndarray) -> dict:
+    L = np.ascontiguousarray(L, np.uint8)
+    R = np.ascontiguousarray(R, np.uint8)
+    H, W = L.shape
+    cs, cd, cn, cnb = orc.cost_top2(cfg, L, R)
+    d32 = np.zeros((H, W), np.float32)
+    b32 = np.zeros((H, W), np.float32)
+    for y in range(H):
+        d, b, _ = orc.solve_row_debug(cfg, cs[y], cd[y], cn[y], cnb[y] if cfg.subpixel else None)
+        d32[y], b32[y] = d, b
+    nb = np.where(cnb == -32768, NONE, cnb.astype(np.float64) / 16384.0)
+    if not cfg.subpixel:
+        nb[:] = NONE
+    cs64 = np.where(cs > -1e29, cs.astype(np.float64), NONE)
+    d64, b64 = orc.solve_f64(cfg, cs64, cd, cn, nb)
+    same = _same_answer(d32, d64, 0.01)
+    both = np.isfinite(d32) & np.isfinite(d64) & same
+    belief = (b32 > -1e29) & (b64 > -1e29)
+    fcs, fcd, fcn, fnb = orc.cost_top2_f64(cfg, L, R)
+    e64, _ = orc.solve_f64(cfg, fcs, fcd, fcn, fnb)
+    return {"solve_agreement": float(same.mean()),
+            "solve_max_disp_diff_px": float(np.abs(d32[both] - d64[both]).max()) if both.any() else 0.0,
+            "solve_max_belief_err": float(np.abs(b32[belief] - b64[belief]).max()) if belief.any() else 0.0,
+            "e2e_agreement_0p5px": float(_same_answer(d32, e64, 0.5).mean()),
+            "e2e_agreement_1px": float(_same_answer(d32, e64, 1.0).mean()),
+            "filled_f32": float(np.isfinite(d32).mean()),
+            "filled_f64": float(np.isfinite(e64).mean()), "iters": int(cfg.iters)}
+
+
 def workloads():
     from doubleeye_b200 import synth
     yield "C1 848x480 D=64 census 9x7", O.default_cfg(dmax=64, iters=10, census_hw=4), \
@@ -88,6 +140,7 @@ def main() -> None:
     for name, cfg, p in workloads():
         t = time.perf_counter()
         s = statement(orc, cfg, p.left, p.right)
+        s.update(solve_statement(orc, cfg, p.left, p.right))
         s["config"] = name
         s["seconds"] = round(time.perf_counter() - t, 1)
         print(json.dumps(s), flush=True)

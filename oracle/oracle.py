@@ -150,6 +150,9 @@ class Oracle:
                                    C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]
         L.or_solve_row_debug.argtypes = [C.POINTER(DeCfg), C.c_int] + [C.c_void_p] * 9
+        L.or_solve_row_f64.argtypes = [C.POINTER(DeCfg), C.c_int] + [C.c_void_p] * 6
+        L.or_cost_top2_f64.argtypes = [C.POINTER(DeCfg), C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_int] + [C.c_void_p] * 4
         L.or_dense.argtypes = [C.POINTER(DeCfg), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                C.c_void_p, C.c_void_p, C.c_void_p]
         L.or_dense_prior.argtypes = [C.POINTER(DeCfg), C.c_void_p, C.c_void_p, C.c_int, C.c_int,
@@ -349,6 +352,36 @@ class Oracle:
             cnb.ctypes.data if cnb is not None else None, disp.ctypes.data,
             margin.ctypes.data, lrc2.ctypes.data, best.ctypes.data, target.ctypes.data)
         return disp, best, target
+
+    def solve_f64(self, cfg: DeCfg, cs, cd, cn, nb):
+        """The row solve in double precision over candidate planes (H, W, 2): cs and nb
+        (the winner's neighbour costs) in score units, -1e300 where missing.
+        Returns (disp, belief) as float64."""
+        H, W = cn.shape
+        cs = np.ascontiguousarray(cs, np.float64)
+        cd = np.ascontiguousarray(cd, np.int32)
+        cn = np.ascontiguousarray(cn, np.int32)
+        nb = np.ascontiguousarray(nb, np.float64)
+        disp = np.zeros((H, W), np.float64)
+        best = np.zeros((H, W), np.float64)
+        for y in range(H):
+            self.lib.or_solve_row_f64(C.byref(cfg), W, cs[y].ctypes.data, cd[y].ctypes.data,
+                                      cn[y].ctypes.data, nb[y].ctypes.data,
+                                      disp[y].ctypes.data, best[y].ctypes.data)
+        return disp, best
+
+    def cost_top2_f64(self, cfg: DeCfg, L, R):
+        """The cost stage with the filter in double precision, unrounded."""
+        L = np.ascontiguousarray(L, np.uint8)
+        R = np.ascontiguousarray(R, np.uint8)
+        H, W = L.shape
+        cs = np.zeros((H, W, 2), np.float64)
+        nb = np.zeros((H, W, 2), np.float64)
+        cd = np.zeros((H, W, 2), np.int32)
+        cn = np.zeros((H, W), np.int32)
+        self.lib.or_cost_top2_f64(C.byref(cfg), L.ctypes.data, R.ctypes.data, W, H,
+                                  cs.ctypes.data, cd.ctypes.data, cn.ctypes.data, nb.ctypes.data)
+        return cs, cd, cn, nb
 
     def dense(self, cfg: DeCfg, L, R, want_cand: bool = True):
         L = np.ascontiguousarray(L, np.uint8)

@@ -15,9 +15,9 @@ CUDA behind a C ABI (include/doubleeye_b200.h).  Modules:
   build        nvcc build of the in-tree library and the de_dense_gpu command line
 """
 from .dense import (CAND_PLANES, Cfg, DenseMatcher, DenseResult, census, confidence,
-                    cost_top2, new_results, pinned_empty, run_dense, run_dense_batch,
-                    run_dense_prior, solve)
+                    cost_top2, fill_holes, new_results, pinned_empty, run_dense,
+                    run_dense_batch, run_dense_prior, solve)
 
 __all__ = ["CAND_PLANES", "Cfg", "DenseMatcher", "DenseResult", "census", "confidence",
-           "cost_top2", "new_results", "pinned_empty", "run_dense", "run_dense_batch",
-           "run_dense_prior", "solve"]
+           "cost_top2", "fill_holes", "new_results", "pinned_empty", "run_dense",
+           "run_dense_batch", "run_dense_prior", "solve"]

@@ -160,6 +160,9 @@ SIGNATURES = {
     "de_server_last_disparity": (C.c_int, [vp, C.c_int, vp, C.c_int, C.c_int]),
     "de_server_destroy": (C.c_int, [vp]),
     "de_dedd_encode_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp, vp]),
+    "de_server_stream_prior": (C.c_int, [vp, C.c_int, C.c_int]),
+    "de_prior_fill_workspace_bytes": (C.c_size_t, [C.c_int, C.c_int]),
+    "de_prior_fill_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, C.c_size_t, vp]),
 }
 
 _lib = None

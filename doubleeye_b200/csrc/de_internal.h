@@ -129,6 +129,10 @@ cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStre
 size_t prior_ws_bytes(int W, int H, int D);
 cudaError_t launch_prior(const DevCfg& cfg, const Batch& b, const float* prior, int band,
                          void* ws, cudaStream_t s);
+// Hole filling of a disparity map for use as a prior (de_fill.cu).
+size_t fill_ws_bytes(int W, int H);
+int fill_holes_dev(const float* src, float* dst, int W, int H, void* ws, size_t ws_bytes,
+                   cudaStream_t s);
 // Sparse path (de_sparse.cu), for the host-pointer context.
 size_t detect_ws_bytes(int W, int H, const de_det_cfg* c);
 int detect_fast_dev(const uint8_t* img, int W, int H, const de_det_cfg* c, de_keypoint* out,

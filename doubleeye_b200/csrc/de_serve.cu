@@ -16,11 +16,16 @@
 //   * completion is signalled from the stream (a host callback), results are copied
 //     out of the pinned mirror, and per-request latency (submit to result) is kept for
 //     the p50/p99 report;
-//   * each camera stream keeps device state: its last two disparity maps (the frame
-//     just delivered and the one in flight), readable without a host round trip by
-//     device consumers and on request by the host;
-//   * results are those of the plain pipeline bit for bit: batching changes which
-//     pairs share a launch, never the arithmetic (each pair's work is independent).
+//   * each camera stream keeps device state: its last two disparity maps (allocated at
+//     the stream's first frame of a size, kept until the server is destroyed),
+//     readable on request by the host;
+//   * a stream can be given a temporal prior (de_server_stream_prior): its frames are
+//     then matched through the prior path (core/tools/de_dense.cpp:797-853, --prior)
+//     with its previous map, hole-filled on the device
+//     (article/coarse_to_fine.py:58-76), as the prior, one at a time and in order;
+//   * results are those of the plain (or prior) pipeline bit for bit: batching changes
+//     which pairs share a launch, never the arithmetic (each pair's work is
+//     independent).
 // The DEDD encoding of the live path (Q4 int16 disparity, -32768 where the matcher
 // declined, u8 confidence zeroed there) is produced on the device with the outputs.
 
@@ -85,6 +90,7 @@ namespace {
 struct Req {
   uint64_t ticket = 0;
   int stream = 0, W = 0, H = 0, dmax = 0;
+  int band = 0;                        // temporal prior band of its stream at admission
   unsigned planes = 0;                 // DE_PLANE_* the client will read
   std::vector<uint8_t> L, R;
   std::vector<float> disp, margin;
@@ -98,25 +104,46 @@ struct Slot {                          // one request's place in a lane's arena
   size_t L, R, disp, margin, conf, q4, qconf;
 };
 
+// Arena of one batch: [inputs | outputs | status words] [plain workspace] [one-at-a-
+// time workspace].  Requests of streams without a prior run as one batched launch
+// set in the plain workspace; requests of streams with a prior run one at a time, in
+// order, reusing the one-at-a-time workspace (a filled prior map, the fill's scratch
+// and the prior path's workspace, or a single pair's dense workspace).
+struct Plan {
+  std::vector<Slot> slots;
+  std::vector<int> plain, seq;         // request indices, in batch order
+  size_t in_end = 0, out_end = 0;      // I/O block: inputs [0, in_end), outputs to out_end
+  size_t status = 0;                   // status words: [0] plain batch, [1 + i] seq[i]
+  size_t io_end = 0;                   // end of the I/O block (the pinned mirror's share)
+  size_t ws_plain = 0, ws_plain_bytes = 0;
+  size_t ws_seq = 0, ws_seq_bytes = 0;
+  size_t total = 0;
+};
+
 struct Lane {
   cudaStream_t s = nullptr;
-  uint8_t* dev = nullptr;              // I/O block, then the pipeline workspace
+  uint8_t* dev = nullptr;              // I/O block, then the pipeline workspaces
   size_t dev_cap = 0;
   uint8_t* pin = nullptr;              // pinned mirror of the I/O block
   size_t pin_cap = 0;
   std::vector<Req*> batch;
-  std::vector<Slot> slots;
-  size_t in_end = 0, out_begin = 0, out_end = 0;
+  Plan plan;
   bool busy = false;
   bool finished = false;               // set by the stream callback
   struct de_server* owner = nullptr;
 };
 
+// Per camera stream, on the device: the last two disparity maps (slot frames & 1 takes
+// frame number `frames`).  Each slot's last write and last host read are events, so a
+// write waits for the slot's previous write and read, whichever lanes issued them.
 struct StreamState {
   int W = 0, H = 0;
-  float* buf[2] = {nullptr, nullptr};  // last two disparity maps on the device
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  uint64_t frames = 0;                 // frames launched
+  float* buf[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};   // last write of the slot
+  cudaEvent_t rd[2] = {nullptr, nullptr};   // last host read of the slot
+  bool read_issued[2] = {false, false};
+  uint64_t frames = 0;                      // maps written since the last size change
+  int band = 0;                             // temporal prior band, 0 = off
 };
 
 }  // namespace
@@ -126,13 +153,24 @@ struct de_server {
   de_server_cfg scfg{};
   int device = 0;
   std::vector<Lane> lanes;
-  std::mutex mu;
+  std::mutex mu;                       // requests, lanes, statistics
   std::condition_variable cv_work;     // new request, finished lane or stop
   std::condition_variable cv_done;     // a request finished
   std::deque<Req*> pending;
   std::unordered_map<uint64_t, Req*> reqs;
   uint64_t next_ticket = 1;
+  // Stream state has its own lock, never held while taking `mu` (order: mu, then
+  // state_mu).  Device work on stream state is enqueued under it, so the order of
+  // writes and reads of a slot is the order they were enqueued in.  Nothing is freed
+  // while the server runs: maps replaced after a size change are retired and freed at
+  // destruction, so a read already enqueued never sees freed memory.
+  std::mutex state_mu;
   std::unordered_map<int, StreamState> streams;
+  std::vector<float*> retired;
+  cudaStream_t state_s = nullptr;      // host reads of stream state
+  std::mutex rd_mu;                    // one host read at a time, through rd_pin
+  float* rd_pin = nullptr;
+  size_t rd_cap = 0;
   std::vector<Req*> pool;              // finished requests kept with their buffers
   std::vector<double> lat;
   uint64_t batches = 0, batched_pairs = 0, completed = 0, failed = 0;
@@ -154,110 +192,202 @@ void CUDART_CB lane_done(void* p) {
   sv->cv_work.notify_all();
 }
 
-// Arena layout of a prospective batch; returns the device bytes needed (I/O block +
-// workspace), and in *out_end the I/O block's size (the pinned mirror's share, plus
-// 256 bytes for the status word).
-size_t plan_batch(const de_server* sv, const std::vector<Req*>& b, std::vector<Slot>* slots,
-                  size_t* in_end, size_t* out_begin, size_t* out_end, size_t* ws_bytes) {
-  std::vector<Slot> s(b.size());
+de_pair pair_of(const Req* r) {
+  de_pair p{};
+  p.L = p.R = reinterpret_cast<const uint8_t*>(1);   // sizing only
+  p.W = r->W;
+  p.H = r->H;
+  p.dmax = r->dmax;
+  return p;
+}
+
+// Arena layout of a prospective batch; false if a pair is outside the pipeline's limits.
+bool plan_batch(const de_server* sv, const std::vector<Req*>& b, Plan* pl) {
+  Plan P;
+  P.slots.resize(b.size());
   size_t o = 0;
   for (size_t i = 0; i < b.size(); ++i) {
     const size_t WH = size_t(b[i]->W) * b[i]->H;
-    s[i].L = o;  o = align256(o + WH);
-    s[i].R = o;  o = align256(o + WH);
+    P.slots[i].L = o;  o = align256(o + WH);
+    P.slots[i].R = o;  o = align256(o + WH);
+    (b[i]->band > 0 ? P.seq : P.plain).push_back(int(i));
   }
-  const size_t ie = o;
+  P.in_end = o;
   for (size_t i = 0; i < b.size(); ++i) {
     const size_t WH = size_t(b[i]->W) * b[i]->H;
-    s[i].disp = o;    o = align256(o + WH * 4);
-    s[i].margin = o;  o = align256(o + WH * 4);
-    s[i].conf = o;    o = align256(o + WH);
-    s[i].q4 = o;      o = align256(o + WH * 2);
-    s[i].qconf = o;   o = align256(o + WH);
+    Slot& s = P.slots[i];
+    s.disp = o;    o = align256(o + WH * 4);
+    s.margin = o;  o = align256(o + WH * 4);
+    s.conf = o;    o = align256(o + WH);
+    s.q4 = o;      o = align256(o + WH * 2);
+    s.qconf = o;   o = align256(o + WH);
   }
-  const size_t oe = o;
-  std::vector<de_pair> pairs(b.size());
-  for (size_t i = 0; i < b.size(); ++i) {
-    pairs[i] = de_pair{};
-    pairs[i].L = pairs[i].R = reinterpret_cast<const uint8_t*>(1);
-    pairs[i].W = b[i]->W;
-    pairs[i].H = b[i]->H;
-    pairs[i].dmax = b[i]->dmax;
+  P.out_end = o;
+  P.status = o;
+  o = align256(o + (1 + P.seq.size()) * sizeof(int));
+  P.io_end = o;
+  std::vector<de_pair> pairs;
+  for (int i : P.plain) pairs.push_back(pair_of(b[i]));
+  if (!pairs.empty() &&
+      de_dense_workspace_bytes(&sv->cfg, pairs.data(), int(pairs.size()), &P.ws_plain_bytes))
+    return false;
+  for (int i : P.seq) {
+    const de_pair p = pair_of(b[i]);
+    size_t dense = 0, prior = 0;
+    if (de_dense_workspace_bytes(&sv->cfg, &p, 1, &dense) ||
+        de_dense_prior_workspace_bytes(&sv->cfg, &p, &prior))
+      return false;
+    const size_t map = align256(size_t(p.W) * p.H * 4);
+    P.ws_seq_bytes = std::max({P.ws_seq_bytes, dense,
+                               map + de::fill_ws_bytes(p.W, p.H) + align256(prior)});
   }
-  size_t ws = 0;
-  if (de_dense_workspace_bytes(&sv->cfg, pairs.data(), int(pairs.size()), &ws)) return ~size_t(0);
-  if (slots) *slots = std::move(s);
-  if (in_end) *in_end = ie;
-  if (out_begin) *out_begin = ie;
-  if (out_end) *out_end = oe;
-  if (ws_bytes) *ws_bytes = ws;
-  return align256(oe) + ws;
+  P.ws_plain = P.io_end;
+  P.ws_seq = align256(P.ws_plain + P.ws_plain_bytes);
+  P.total = P.ws_seq + P.ws_seq_bytes;
+  *pl = std::move(P);
+  return true;
 }
 
-// Enqueues one batch on a free lane.  Called by the worker without the lock held;
-// the requests are already owned by the lane.
+de_pair device_pair(const Lane& l, const Req* r, const Slot& s) {
+  de_pair p{};
+  p.L = l.dev + s.L;
+  p.R = l.dev + s.R;
+  p.W = r->W;
+  p.H = r->H;
+  p.dmax = r->dmax;
+  p.disp = reinterpret_cast<float*>(l.dev + s.disp);
+  p.margin = reinterpret_cast<float*>(l.dev + s.margin);
+  p.conf = l.dev + s.conf;
+  return p;
+}
+
+// The stream's map slot for this request's frame, (re)allocated at a size change;
+// called on the worker thread with state_mu held.  A replaced map is retired, not
+// freed (a read may still be queued on it).
+int ensure_state(de_server* sv, StreamState* st, int W, int H) {
+  for (int k = 0; k < 2; ++k) {
+    if (!st->ev[k] && cudaEventCreateWithFlags(&st->ev[k], cudaEventDisableTiming) != cudaSuccess)
+      return de::set_error(DE_ERR_CUDA, "stream state event");
+    if (!st->rd[k] && cudaEventCreateWithFlags(&st->rd[k], cudaEventDisableTiming) != cudaSuccess)
+      return de::set_error(DE_ERR_CUDA, "stream state event");
+  }
+  if (st->W == W && st->H == H && st->buf[0]) return DE_OK;
+  float* nb[2] = {nullptr, nullptr};
+  const size_t bytes = size_t(W) * H * 4;
+  cudaError_t e = cudaMalloc(&nb[0], bytes);
+  if (e == cudaSuccess) e = cudaMalloc(&nb[1], bytes);
+  if (e != cudaSuccess) {
+    if (nb[0]) sv->retired.push_back(nb[0]);
+    return de::set_error(DE_ERR_OOM, "stream state: %s", cudaGetErrorString(e));
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (st->buf[k]) sv->retired.push_back(st->buf[k]);
+    st->buf[k] = nb[k];
+  }
+  st->W = W;
+  st->H = H;
+  st->frames = 0;
+  return DE_OK;
+}
+
+// This frame's disparity map into the stream's next slot, after the slot's previous
+// write and read.
+int record_state(de_server* sv, cudaStream_t s, const Req* r, const float* disp) {
+  std::lock_guard<std::mutex> lk(sv->state_mu);
+  StreamState* st = &sv->streams[r->stream];
+  if (int rc = ensure_state(sv, st, r->W, r->H)) return rc;
+  const int k = int(st->frames & 1);
+  cudaError_t e = cudaStreamWaitEvent(s, st->ev[k], 0);
+  if (e == cudaSuccess && st->read_issued[k]) e = cudaStreamWaitEvent(s, st->rd[k], 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(st->buf[k], disp, size_t(r->W) * r->H * 4, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaEventRecord(st->ev[k], s);
+  if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "state: %s", cudaGetErrorString(e));
+  ++st->frames;
+  return DE_OK;
+}
+
+// The previous map of a prior stream, if it has one of this size: its device address,
+// with `s` made to wait for its write.  nullptr: match this frame without a prior.
+const float* previous_map(de_server* sv, cudaStream_t s, const Req* r) {
+  std::lock_guard<std::mutex> lk(sv->state_mu);
+  auto it = sv->streams.find(r->stream);
+  if (it == sv->streams.end()) return nullptr;
+  StreamState& st = it->second;
+  if (st.frames == 0 || st.W != r->W || st.H != r->H) return nullptr;
+  const int k = int((st.frames - 1) & 1);
+  if (cudaStreamWaitEvent(s, st.ev[k], 0) != cudaSuccess) return nullptr;
+  return st.buf[k];
+}
+
+// Enqueues one batch on a free lane.  Called by the worker without `mu` held; the
+// requests are already owned by the lane.
 int launch(de_server* sv, Lane& l) {
-  size_t ws = 0;
-  plan_batch(sv, l.batch, &l.slots, &l.in_end, &l.out_begin, &l.out_end, &ws);
-  const size_t ws_off = align256(l.out_end);
-  std::vector<de_pair> dp(l.batch.size());
+  if (!plan_batch(sv, l.batch, &l.plan)) return de::set_error(DE_ERR_ARG, "batch plan");
+  const Plan& P = l.plan;
   std::vector<de::HostCopy> jobs;
   for (size_t i = 0; i < l.batch.size(); ++i) {
     Req* r = l.batch[i];
-    const Slot& s = l.slots[i];
     const size_t WH = size_t(r->W) * r->H;
-    jobs.push_back({l.pin + s.L, r->L.data(), WH});
-    jobs.push_back({l.pin + s.R, r->R.data(), WH});
-    dp[i] = de_pair{};
-    dp[i].L = l.dev + s.L;
-    dp[i].R = l.dev + s.R;
-    dp[i].W = r->W;
-    dp[i].H = r->H;
-    dp[i].dmax = r->dmax;
-    dp[i].disp = reinterpret_cast<float*>(l.dev + s.disp);
-    dp[i].margin = reinterpret_cast<float*>(l.dev + s.margin);
-    dp[i].conf = l.dev + s.conf;
+    jobs.push_back({l.pin + P.slots[i].L, r->L.data(), WH});
+    jobs.push_back({l.pin + P.slots[i].R, r->R.data(), WH});
     r->t_launch = now_ms();
   }
   de::parallel_copy(jobs);
-  cudaError_t e = cudaMemcpyAsync(l.dev, l.pin, l.in_end, cudaMemcpyHostToDevice, l.s);
+  cudaError_t e = cudaMemcpyAsync(l.dev, l.pin, P.in_end, cudaMemcpyHostToDevice, l.s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(l.dev + P.status, 0, (1 + P.seq.size()) * sizeof(int), l.s);
   if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
-  int rc = de_dense_dev(&sv->cfg, dp.data(), int(dp.size()), l.dev + ws_off, ws, l.s);
-  if (rc) return rc;
-  for (size_t i = 0; i < l.batch.size(); ++i) {
+  int* status = reinterpret_cast<int*>(l.dev + P.status);
+  auto finish = [&](int i) -> int {                  // DEDD planes and stream state
     Req* r = l.batch[i];
-    const Slot& s = l.slots[i];
-    rc = de::dedd_encode_dev(reinterpret_cast<float*>(l.dev + s.disp), l.dev + s.conf, r->W,
-                             r->H, reinterpret_cast<int16_t*>(l.dev + s.q4), l.dev + s.qconf,
-                             l.s);
-    if (rc) return rc;
-    // per-stream device state: this frame's disparity into the stream's next buffer
-    std::lock_guard<std::mutex> lk(sv->mu);
-    StreamState* st = &sv->streams[r->stream];
-    const size_t bytes = size_t(r->W) * r->H * 4;
-    if (st->W != r->W || st->H != r->H) {
-      for (int k = 0; k < 2; ++k) {
-        if (st->buf[k]) cudaFree(st->buf[k]);
-        st->buf[k] = nullptr;
-        if (!st->ev[k]) cudaEventCreateWithFlags(&st->ev[k], cudaEventDisableTiming);
-      }
-      e = cudaMalloc(&st->buf[0], bytes);
-      if (e == cudaSuccess) e = cudaMalloc(&st->buf[1], bytes);
-      if (e != cudaSuccess)
-        return de::set_error(DE_ERR_OOM, "stream state: %s", cudaGetErrorString(e));
-      st->W = r->W;
-      st->H = r->H;
+    const Slot& s = P.slots[i];
+    if (int rc = de::dedd_encode_dev(reinterpret_cast<float*>(l.dev + s.disp), l.dev + s.conf,
+                                     r->W, r->H, reinterpret_cast<int16_t*>(l.dev + s.q4),
+                                     l.dev + s.qconf, l.s))
+      return rc;
+    return record_state(sv, l.s, r, reinterpret_cast<float*>(l.dev + s.disp));
+  };
+  // streams without a prior: one batched launch set
+  if (!P.plain.empty()) {
+    std::vector<de_pair> dp;
+    for (int i : P.plain) dp.push_back(device_pair(l, l.batch[i], P.slots[i]));
+    if (int rc = de_dense_dev(&sv->cfg, dp.data(), int(dp.size()), l.dev + P.ws_plain,
+                              P.ws_plain_bytes, l.s))
+      return rc;
+    e = cudaMemcpyAsync(status, l.dev + P.ws_plain, sizeof(int), cudaMemcpyDeviceToDevice, l.s);
+    if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "status: %s", cudaGetErrorString(e));
+    for (int i : P.plain)
+      if (int rc = finish(i)) return rc;
+  }
+  // streams with a prior: one at a time, each after its stream's previous frame
+  for (size_t q = 0; q < P.seq.size(); ++q) {
+    const int i = P.seq[q];
+    const Req* r = l.batch[i];
+    const de_pair dp = device_pair(l, r, P.slots[i]);
+    uint8_t* ws = l.dev + P.ws_seq;
+    const float* prev = previous_map(sv, l.s, r);
+    int rc;
+    if (prev) {
+      float* prior = reinterpret_cast<float*>(ws);
+      const size_t map = align256(size_t(r->W) * r->H * 4);
+      const size_t fill = de::fill_ws_bytes(r->W, r->H);
+      rc = de::fill_holes_dev(prev, prior, r->W, r->H, ws + map, fill, l.s);
+      if (!rc) rc = de_dense_prior_dev(&sv->cfg, &dp, prior, r->band, ws + map + fill,
+                                       P.ws_seq_bytes - map - fill, l.s);
+      ws += map + fill;                               // the status word's workspace
+    } else {
+      rc = de_dense_dev(&sv->cfg, &dp, 1, ws, P.ws_seq_bytes, l.s);
     }
-    const int k = int(st->frames & 1);
-    e = cudaMemcpyAsync(st->buf[k], l.dev + s.disp, bytes, cudaMemcpyDeviceToDevice, l.s);
-    if (e == cudaSuccess) e = cudaEventRecord(st->ev[k], l.s);
-    if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "state: %s", cudaGetErrorString(e));
-    ++st->frames;
+    if (rc) return rc;
+    e = cudaMemcpyAsync(status + 1 + q, ws, sizeof(int), cudaMemcpyDeviceToDevice, l.s);
+    if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "status: %s", cudaGetErrorString(e));
+    if ((rc = finish(i))) return rc;
   }
   // only the planes each request asked for come back
   for (size_t i = 0; i < l.batch.size() && e == cudaSuccess; ++i) {
     const Req* r = l.batch[i];
-    const Slot& s = l.slots[i];
+    const Slot& s = P.slots[i];
     const size_t WH = size_t(r->W) * r->H;
     const struct { unsigned bit; size_t off, bytes; } planes[] = {
         {DE_PLANE_DISP, s.disp, WH * 4}, {DE_PLANE_MARGIN, s.margin, WH * 4},
@@ -266,9 +396,9 @@ int launch(de_server* sv, Lane& l) {
       if ((r->planes & pl.bit) && e == cudaSuccess)
         e = cudaMemcpyAsync(l.pin + pl.off, l.dev + pl.off, pl.bytes, cudaMemcpyDeviceToHost, l.s);
   }
-  // the pipeline's status word (set by a bounded device wait that ran out)
+  // the status words (a bounded device wait that ran out sets one)
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(l.pin + align256(l.out_end), l.dev + ws_off, sizeof(int),
+    e = cudaMemcpyAsync(l.pin + P.status, status, (1 + P.seq.size()) * sizeof(int),
                         cudaMemcpyDeviceToHost, l.s);
   if (e == cudaSuccess) e = cudaLaunchHostFunc(l.s, lane_done, &l);
   if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "download: %s", cudaGetErrorString(e));
@@ -277,13 +407,16 @@ int launch(de_server* sv, Lane& l) {
 
 // Copies a finished lane's results into its requests.  Lock held.
 void deliver(de_server* sv, Lane& l) {
-  int word = 0;
-  std::memcpy(&word, l.pin + align256(l.out_end), sizeof(int));
-  const int status = word ? DE_ERR_TIMEOUT : 0;
+  const Plan& P = l.plan;
+  std::vector<int> words(1 + P.seq.size());
+  std::memcpy(words.data(), l.pin + P.status, words.size() * sizeof(int));
+  std::vector<int> word_of(l.batch.size(), words[0]);
+  for (size_t q = 0; q < P.seq.size(); ++q) word_of[P.seq[q]] = words[1 + q];
   const double t = now_ms();
   for (size_t i = 0; i < l.batch.size(); ++i) {
     Req* r = l.batch[i];
-    const Slot& s = l.slots[i];
+    const Slot& s = P.slots[i];
+    const int status = word_of[i] ? DE_ERR_TIMEOUT : 0;
     const size_t WH = size_t(r->W) * r->H;
     auto take = [&](unsigned bit, auto& v, size_t off, size_t esz) {
       if (!(r->planes & bit)) return;
@@ -337,10 +470,15 @@ void worker_main(de_server* sv) {
       // admit first come first served while the batch fits the lane
       std::vector<Req*> b;
       while (!sv->pending.empty() && int(b.size()) < sv->scfg.max_batch) {
-        b.push_back(sv->pending.front());
-        size_t io = 0;
-        const size_t need = plan_batch(sv, b, nullptr, nullptr, nullptr, &io, nullptr);
-        if (need > l.dev_cap || align256(io) + 256 > l.pin_cap) {
+        Req* front = sv->pending.front();
+        {
+          std::lock_guard<std::mutex> sl(sv->state_mu);
+          auto it = sv->streams.find(front->stream);
+          front->band = it == sv->streams.end() ? 0 : it->second.band;
+        }
+        b.push_back(front);
+        Plan plan;
+        if (!plan_batch(sv, b, &plan) || plan.total > l.dev_cap || plan.io_end > l.pin_cap) {
           b.pop_back();
           if (b.empty()) {                       // alone it does not fit: refuse it
             Req* r = sv->pending.front();
@@ -439,6 +577,10 @@ int de_server_create(const de_cfg* cfg, const de_server_cfg* scfg, de_server** o
     }
     l.dev_cap = per;
     l.pin_cap = pin;
+  }
+  if (cudaStreamCreateWithFlags(&sv->state_s, cudaStreamNonBlocking) != cudaSuccess) {
+    de_server_destroy(sv);
+    return de::set_error(DE_ERR_CUDA, "server state stream");
   }
   sv->worker = std::thread(worker_main, sv);
   *out = sv;
@@ -546,26 +688,55 @@ int de_server_reset_stats(de_server* sv) {
   return DE_OK;
 }
 
+int de_server_stream_prior(de_server* sv, int stream, int band) {
+  if (!sv) return de::set_error(DE_ERR_ARG, "server is NULL");
+  if (band < 0 || band > DE_MAX_D) return de::set_error(DE_ERR_ARG, "band %d outside 0..%d",
+                                                        band, DE_MAX_D);
+  if (band > 0 && (sv->cfg.census_hw != 3 || sv->cfg.census_hh != 3))
+    return de::set_error(DE_ERR_ARG, "the prior path is the reference's 7x7-census path");
+  std::lock_guard<std::mutex> lk(sv->state_mu);
+  sv->streams[stream].band = band;
+  return DE_OK;
+}
+
 int de_server_last_disparity(de_server* sv, int stream, float* host, int W, int H) {
-  if (!sv || !host) return de::set_error(DE_ERR_ARG, "NULL argument");
-  float* src = nullptr;
-  cudaEvent_t ev = nullptr;
+  if (!sv || !host || W < 1 || H < 1) return de::set_error(DE_ERR_ARG, "bad argument");
+  const size_t bytes = size_t(W) * H * 4;
+  std::lock_guard<std::mutex> rl(sv->rd_mu);         // one reader at a time owns rd_pin
+  cudaSetDevice(sv->device);
+  if (sv->rd_cap < bytes) {
+    if (sv->rd_pin) cudaFreeHost(sv->rd_pin);
+    sv->rd_pin = nullptr;
+    sv->rd_cap = 0;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&sv->rd_pin), bytes, cudaHostAllocDefault) !=
+        cudaSuccess)
+      return de::set_error(DE_ERR_OOM, "state read buffer");
+    sv->rd_cap = bytes;
+  }
+  cudaEvent_t done = nullptr;
   {
-    std::lock_guard<std::mutex> lk(sv->mu);
+    // the copy is enqueued under state_mu, after the slot's write and before the
+    // slot's next write (which waits for this read's event)
+    std::lock_guard<std::mutex> lk(sv->state_mu);
     auto it = sv->streams.find(stream);
     if (it == sv->streams.end() || it->second.frames == 0)
       return de::set_error(DE_ERR_ARG, "stream %d has no frame yet", stream);
     StreamState& st = it->second;
     if (st.W != W || st.H != H)
       return de::set_error(DE_ERR_ARG, "stream %d is %dx%d", stream, st.W, st.H);
-    const int k = int((st.frames - 1) & 1);       // the newest launched frame
-    src = st.buf[k];
-    ev = st.ev[k];
+    const int k = int((st.frames - 1) & 1);          // the newest launched frame
+    cudaError_t e = cudaStreamWaitEvent(sv->state_s, st.ev[k], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(sv->rd_pin, st.buf[k], bytes, cudaMemcpyDeviceToHost, sv->state_s);
+    if (e == cudaSuccess) e = cudaEventRecord(st.rd[k], sv->state_s);
+    if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "state read: %s", cudaGetErrorString(e));
+    st.read_issued[k] = true;
+    done = st.rd[k];
   }
-  cudaSetDevice(sv->device);
-  cudaError_t e = cudaEventSynchronize(ev);
-  if (e == cudaSuccess) e = cudaMemcpy(host, src, size_t(W) * H * 4, cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "state read: %s", cudaGetErrorString(e));
+  // rd events are recorded only by readers, and readers are serialised by rd_mu
+  if (cudaEventSynchronize(done) != cudaSuccess)
+    return de::set_error(DE_ERR_CUDA, "state read: %s", cudaGetErrorString(cudaGetLastError()));
+  std::memcpy(host, sv->rd_pin, bytes);
   return DE_OK;
 }
 
@@ -584,11 +755,16 @@ int de_server_destroy(de_server* sv) {
     if (l.pin) cudaFreeHost(l.pin);
     if (l.s) cudaStreamDestroy(l.s);
   }
+  if (sv->state_s) cudaStreamSynchronize(sv->state_s);
   for (auto& kv : sv->streams)
     for (int k = 0; k < 2; ++k) {
       if (kv.second.buf[k]) cudaFree(kv.second.buf[k]);
       if (kv.second.ev[k]) cudaEventDestroy(kv.second.ev[k]);
+      if (kv.second.rd[k]) cudaEventDestroy(kv.second.rd[k]);
     }
+  for (float* p : sv->retired) cudaFree(p);
+  if (sv->rd_pin) cudaFreeHost(sv->rd_pin);
+  if (sv->state_s) cudaStreamDestroy(sv->state_s);
   for (auto& kv : sv->reqs) delete kv.second;
   for (Req* r : sv->pool) delete r;
   delete sv;

@@ -158,6 +158,27 @@ def run_dense_prior(left, right, prior, cfg: Optional[DeCfg] = None, *, band: in
     return res
 
 
+def fill_holes(disp, device: int = 0) -> np.ndarray:
+    """A disparity map with its holes filled, ready to serve as a prior: the
+    reference's ``fill`` (article/coarse_to_fine.py:58-76; iterated 4-neighbour
+    averaging with wrap-around, at most 128 sweeps, what is left becomes 0), run on
+    the GPU by de_prior_fill_dev."""
+    torch = _torch()
+    d = np.ascontiguousarray(disp, np.float32)
+    if d.ndim != 2:
+        raise ValueError("the map must be 2-D")
+    H, W = d.shape
+    dev = torch.device("cuda", device)
+    with torch.cuda.device(dev):
+        src = torch.from_numpy(d).to(dev)
+        dst = torch.empty_like(src)
+        ws = torch.empty(int(lib().de_prior_fill_workspace_bytes(W, H)), dtype=torch.uint8,
+                         device=dev)
+        check(lib().de_prior_fill_dev(src.data_ptr(), dst.data_ptr(), W, H, ws.data_ptr(),
+                                      ws.numel(), _stream_handle()))
+        return dst.cpu().numpy()
+
+
 # --------------------------------------------------------------------------------------
 # Device-tensor API (torch for device memory and streams; the work is the C ABI's)
 

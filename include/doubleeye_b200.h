@@ -274,6 +274,17 @@ DE_API int de_dense_prior_workspace_bytes(const de_cfg* cfg, const de_pair* pair
 DE_API int de_dense_prior_dev(const de_cfg* cfg, const de_pair* pair, const float* prior,
                               int band, void* workspace, size_t bytes, void* stream);
 
+/* Hole filling of a disparity map so it can serve as a prior (a prior with holes is
+ * refused): the reference's fill (article/coarse_to_fine.py:58-76), iterated
+ * 4-neighbour averaging.  Up to 128 sweeps; in each, every non-finite pixel with a
+ * finite 4-neighbour (neighbours wrap around the edges) becomes the float32 mean of
+ * those neighbours, summed left, right, up, down; sweeps stop when one changes
+ * nothing, and what is left non-finite becomes 0.  src and dst are W x H float32 on
+ * the device (src is not modified); workspace >= de_prior_fill_workspace_bytes. */
+DE_API size_t de_prior_fill_workspace_bytes(int W, int H);
+DE_API int de_prior_fill_dev(const float* src, float* dst, int W, int H, void* workspace,
+                             size_t bytes, void* stream);
+
 /* ---- a batch captured as a CUDA graph ---------------------------------------- */
 /* Captures de_dense_dev(cfg, pairs, n, workspace) once; each de_graph_launch replays
  * the whole batch (status reset + four kernels) as one launch on the given stream,
@@ -384,6 +395,13 @@ DE_API int de_server_wait(de_server* sv, unsigned long long ticket, int timeout_
                           uint8_t* qconf, double* latency_ms);
 DE_API int de_server_stats(de_server* sv, de_server_report* out);
 DE_API int de_server_reset_stats(de_server* sv);
+/* Temporal prior for one camera stream (band > 0; 0 turns it off): each of its frames
+ * after the first of a size is matched through the prior path (de_dense_prior_dev)
+ * with the stream's previous disparity map, hole-filled by de_prior_fill_dev, as the
+ * prior; both maps stay on the device.  The frames of such a stream run in submission
+ * order, each after the one before it.  Needs the 7x7 census.  Applies to frames
+ * admitted after the call. */
+DE_API int de_server_stream_prior(de_server* sv, int stream, int band);
 /* The newest disparity map a stream has on the device (waits for it), W x H f32. */
 DE_API int de_server_last_disparity(de_server* sv, int stream, float* host, int W, int H);
 DE_API int de_server_destroy(de_server* sv);

@@ -118,6 +118,33 @@ def reference_root() -> str:
     return root
 
 
+def fill_prior(dc: np.ndarray, max_sweeps: int = 128) -> np.ndarray:
+    """Hole filling of a disparity map before it serves as a prior, restating the
+    reference's ``fill`` (article/coarse_to_fine.py:58-76) in float32: each sweep gives
+    every non-finite pixel with a finite 4-neighbour (wrapping around the edges) the
+    mean of those neighbours, accumulated left, right, up, down; sweeps stop when none
+    changes anything or after max_sweeps; non-finite leftovers become 0."""
+    d = np.array(dc, np.float32, copy=True)
+    for _ in range(max_sweeps):
+        hole = ~np.isfinite(d)
+        if not hole.any():
+            break
+        total = np.zeros_like(d)
+        count = np.zeros_like(d)
+        # (rows, cols) shifts: the neighbour to the left, right, above, below
+        for sy, sx in ((0, 1), (0, -1), (1, 0), (-1, 0)):
+            nb = np.roll(d, (sy, sx), axis=(0, 1))
+            good = np.isfinite(nb)
+            total[good] += nb[good]
+            count[good] += 1
+        upd = hole & (count > 0)
+        if not upd.any():
+            break
+        d[upd] = total[upd] / count[upd]
+    d[~np.isfinite(d)] = 0.0
+    return d
+
+
 def build(ref: bool = False) -> None:
     """Build liboracle.so (and _ref/ when asked and the reference tree exists)."""
     targets = ["oracle"] + (["ref"] if ref else [])

@@ -9,6 +9,7 @@ import os
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from oracle.oracle import DeCfg
 from parity import candidates_from_cand6, same_f32, tie_aware_disp
 
@@ -153,3 +154,14 @@ def test_packed_top2_semantics():
             rb1 = (r[1] >> 8) - 32768 if r[1] else -32768
             ri1 = 255 - (r[1] & 255) if r[1] else -1
             assert (rb0, ri0, rb1, ri1) == (b0, i0, b1, i1)
+
+
+def test_fill_prior_matches_reference_fill(golden_dir):
+    """The prior hole fill against the reference's own fill
+    (article/coarse_to_fine.py:58-76), bit for bit."""
+    z = np.load(os.path.join(golden_dir, "fill.npz"))
+    names = sorted({k[:-3] for k in z.files if k.endswith("_in")})
+    assert len(names) >= 6
+    for n in names:
+        got = O.fill_prior(z[n + "_in"])
+        assert got.tobytes() == z[n + "_out"].tobytes(), n

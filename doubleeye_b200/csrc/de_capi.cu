@@ -128,8 +128,7 @@ size_t pair_workspace_bytes(int W, int H, int D, bool lrc) {
   size_t s = 0;
   s += align_up(size_t(H) * cpitch_of(W) * 8) * 2;    // census words L, R
   s += align_up(size_t(H) * apitch_of(W) * 2);        // ax
-  s += align_up(size_t(H) * apitch_of(W) * 2);        // ay
-  s += align_up(size_t(H) * 4);                       // row progress flags
+  s += align_up(WH * 2);                              // ay
   s += align_up(WH * size_t(dpad_of(D)) * 2);     // filtered volume
   s += align_up(WH * 4) * 3;                      // key0, key1, nb
   if (lrc) s += align_up(WH * 4);                 // reverse-match keys
@@ -146,8 +145,7 @@ void carve_pair(DevPair* p, void* ws, int W, int H, int D, int dmin, bool lrc) {
   p->cwL = reinterpret_cast<uint64_t*>(take(size_t(H) * p->cpitch * 8));
   p->cwR = reinterpret_cast<uint64_t*>(take(size_t(H) * p->cpitch * 8));
   p->ax = reinterpret_cast<uint16_t*>(take(size_t(H) * p->apitch * 2));
-  p->ay = reinterpret_cast<uint16_t*>(take(size_t(H) * p->apitch * 2));
-  p->vprog = reinterpret_cast<int*>(take(size_t(H) * 4));
+  p->ay = reinterpret_cast<uint16_t*>(take(WH * 2));
   p->vol = reinterpret_cast<int16_t*>(take(WH * size_t(dpad_of(D)) * 2));
   p->key0 = reinterpret_cast<uint32_t*>(take(WH * 4));
   p->key1 = reinterpret_cast<uint32_t*>(take(WH * 4));

@@ -15,16 +15,14 @@
 //   k_rows    one CTA per image row, a thread per PAIR of adjacent disparities
 //             (int16x2 in one 32-bit register): graded score fused with the
 //             horizontal forward pass, then the backward pass, both sequential in
-//             x as integer rounding demands, and the vertical forward step applied
-//             to each finished chunk against the previous row's stored chunk (rows
-//             taken as tickets in order; a row waits on a per-row progress flag);
-//             the row's census words live in shared memory, the forward result
-//             comes back through a ring of bulk copies.
-//   k_cols    a column is a group of lanes, each lane KT disparities: the vertical
-//             backward pass over the stored forward values, fused with the top-2
-//             (packed keys, a butterfly over the group) and the winner's neighbour
-//             costs; rows stream through per-lane register rings, with no block-
-//             wide step.
+//             x as integer rounding demands; the row's census words live in
+//             shared memory, the forward result comes back through a ring of bulk
+//             copies.
+//   k_cols    a column is a group of lanes, each lane KT disparities: vertical
+//             forward pass written in place, vertical backward pass fused with the
+//             top-2 (packed keys, a butterfly over the group) and the winner's
+//             neighbour costs; rows stream through per-lane register rings, with
+//             no block-wide step.
 //   k_solve   one CTA per row: candidate buckets by right pixel, damped max-sum
 //             iterations, belief, and the one-to-one claim done in parallel as a
 //             per-right-pixel arg-max (each pixel claims exactly one right pixel,
@@ -63,6 +61,7 @@ __device__ __forceinline__ int32_t rf_step(int32_t c, int32_t f, int32_t a) {
   return c + ((a * (f - c) + (1 << 14)) >> 15);
 }
 
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
 __device__ __forceinline__ uint32_t pack2(int32_t lo, int32_t hi) {
   return (uint32_t(uint16_t(lo))) | (uint32_t(hi) << 16);
@@ -100,16 +99,6 @@ __device__ __forceinline__ void census_generic(const uint8_t (*sL)[kCTX + 2 * kM
     }
 }
 
-// The row kernel's per-launch state, reset by the census kernel that precedes it: the
-// pair's row progress flags (by the pair's first tile) and the ticket counters (by the
-// launch's first CTA).
-__device__ __forceinline__ void reset_row_state(const Batch& b, const DevPair& P, int item,
-                                                int t, int tid, int nthreads) {
-  if (t == 0 && P.vprog)
-    for (int i = tid; i < P.H; i += nthreads) P.vprog[i] = 0;
-  if (item == 0 && b.err && tid < 8) b.err[kTicketBase + tid] = 0;
-}
-
 // Any window up to 9x9 (runtime half-widths), one pixel a thread.
 __global__ void __launch_bounds__(kCTX * kCTY) k_census_generic(DevCfg cfg, Batch b) {
   __shared__ uint8_t sL[kCTY + 2 * kMaxHalf][kCTX + 2 * kMaxHalf];
@@ -123,7 +112,6 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census_generic(DevCfg cfg, Batc
   const int tilesX = (W + kCTX - 1) / kCTX;
   const int x0 = (t % tilesX) * kCTX, y0 = (t / tilesX) * kCTY;
   const int tid = threadIdx.y * kCTX + threadIdx.x;
-  reset_row_state(b, P, item, t, tid, kCTX * kCTY);
   for (int i = tid; i < 256; i += kCTX * kCTY) srf[i] = cfg.rf[i];
   constexpr int TW = kCTX + 2 * kMaxHalf, TH = kCTY + 2 * kMaxHalf;
   for (int i = tid; i < TW * TH; i += kCTX * kCTY) {
@@ -150,7 +138,7 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census_generic(DevCfg cfg, Batc
   P.cwR[size_t(y) * P.cpitch + x] = wr;
   const int c = sL[cy][cx];
   P.ax[size_t(y) * P.apitch + P.lpad + x] = x > 0 ? srf[abs(c - int(sL[cy][cx - 1]))] : srf[0];
-  P.ay[size_t(y) * P.apitch + x] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
+  P.ay[size_t(y) * W + x] = y > 0 ? srf[abs(c - int(sL[cy - 1][cx]))] : srf[0];
 }
 
 // k_census_rows<HW>: the (2 HW + 1) x 7 census (7x7, the default, and 9x7), NR
@@ -182,7 +170,6 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census_rows(DevCfg cfg, Batch b
   const int tilesX = (W + kCTX - 1) / kCTX;
   const int x0 = (t % tilesX) * kCTX, y0 = (t / tilesX) * kC2Y;
   const int tid = threadIdx.y * kCTX + threadIdx.x;
-  reset_row_state(b, P, item, t, tid, kCTX * kCTY);
   for (int i = tid; i < 256; i += kCTX * kCTY) srf[i] = cfg.rf[i];
   constexpr int TW = kCTX + 2 * kMaxHalf, TH = kC2Y + 2 * kMaxHalf;
   for (int i = tid; i < TW * TH; i += kCTX * kCTY) {
@@ -236,7 +223,7 @@ __global__ void __launch_bounds__(kCTX * kCTY) k_census_rows(DevCfg cfg, Batch b
     P.cwR[size_t(y) * P.cpitch + x] = wr;
     const int c = int(cl[i]);
     P.ax[size_t(y) * P.apitch + P.lpad + x] = x > 0 ? srf[abs(c - int(sL[cyy][cx - 1]))] : srf[0];
-    P.ay[size_t(y) * P.apitch + x] = y > 0 ? srf[abs(c - int(sL[cyy - 1][cx]))] : srf[0];
+    P.ay[size_t(y) * W + x] = y > 0 ? srf[abs(c - int(sL[cyy - 1][cx]))] : srf[0];
   }
 }
 
@@ -320,60 +307,13 @@ __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async;" ::: "memory");
 }
 
-// Progress flags between the rows of a pair: the row kernel of image row y publishes
-// how many backward chunks of its vertical forward values are stored, and row y + 1
-// waits for the chunk it needs.  Release/acquire at GPU scope; the data itself is read
-// through L2 (ld.global.cg).
-__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
-  int v;
-  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_gpu(int* p, int v) {
-  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-constexpr int kRowWaitLimit = 1 << 20;               // polls of a progress flag
-// Waits until *flag >= need.  Bounded: a wait that runs out (or a status word already
-// set by another) records status 2 and returns, so a fault elsewhere cannot hang the
-// grid; the launch's results are then invalid and the host reports DE_ERR_TIMEOUT.
-__device__ __forceinline__ void wait_progress(const int* flag, int need, int* err) {
-  if (ld_acquire_gpu(flag) >= need) return;
-  for (int i = 0; i < kRowWaitLimit; ++i) {
-    __nanosleep(64);
-    if (ld_acquire_gpu(flag) >= need) return;
-    if ((i & 255) == 255 && err && *reinterpret_cast<volatile int*>(err)) return;
-  }
-  if (err) atomicExch(err, 2);
-}
-
-// Ticket -> (pair, image row): the launch's row order (Batch::seg_*).
-__device__ __forceinline__ int ticket_row(const Batch& b, int t, int hh, int* y) {
-  int lo = 0, hi = b.seg_n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (b.seg_t[mid] <= t) lo = mid; else hi = mid - 1;
-  }
-  const int off = t - b.seg_t[lo], c = b.seg_c[lo];
-  *y = hh + b.seg_r[lo] + off / c;
-  return b.ord_pair[off % c];
-}
-
-// One row per CTA iteration; rows are taken as tickets from a counter, in the launch's
-// row order, so every row a CTA waits for was taken before its own by a CTA that is
-// already running (the grid makes progress whatever the residency).  All pairs of a
+// One row per CTA iteration (the grid is persistent over rows); all pairs of a
 // launch share Dpad = 64 G, so strides and chunk sizes are compile-time.  The row's
-// census words arrive by bulk copy into a single buffer that is refilled for the next
-// row while this row's backward pass runs (only the forward pass reads them); the x-
-// and y-coefficients, read by the backward pass, are double-buffered.  Forward results
-// go to the volume with plain stores; the backward pass brings them back through a
-// ring of bulk copies, so no thread waits on a global load for them.
-//
-// The vertical forward pass (core/tools/de_dense.cpp:490-497) is fused into the
-// backward pass: as the horizontal value H(y, x) of a chunk is finished, the stored
-// value becomes V(y, x) = H(y, x) + ay(y, x) * (V(y - 1, x) - H(y, x)) (the same
-// rounding step), with V(y - 1, x) read from the previous row's stored chunk once that
-// row has published it.  Row hh - 1 is all zero, so row hh needs no previous row.  The
-// column kernel then runs only the vertical backward pass.
+// census words arrive by bulk copy into a single buffer that is refilled for the
+// next row while this row's backward pass runs (only the forward pass reads them);
+// the x-coefficients, read by both passes, are double-buffered.  Forward results go
+// to the volume with plain stores; the backward pass brings them back through a
+// ring of bulk copies, so no thread waits on a global load.
 template <bool PACKED, int TS, int G>
 __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
   constexpr int DP = 64 * G;                          // Dpad
@@ -382,8 +322,7 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
   constexpr int NS = 3;                               // backward ring depth
   constexpr size_t STAGE = size_t(CH) * DP * 2;
   extern __shared__ __align__(128) uint8_t smem[];
-  __shared__ __align__(8) uint64_t bars[4 + NS];      // census, coefficients[2], spare, ring
-  __shared__ int s_ticket[2];
+  __shared__ __align__(8) uint64_t bars[4 + NS];      // census, ax[2], spare, ring
   int cpm = 0, apm = 0, maxW = 0;
   for (int i = 0; i < b.n; ++i) {
     cpm = max(cpm, b.p[i].cpitch);
@@ -392,19 +331,15 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
   }
   uint8_t* tabp = smem;
   uint8_t* cbuf = tabp + ScoreTable<TS, 1>::bytes();                 // L | R words
-  uint8_t* abuf = cbuf + size_t(cpm) * 16;                            // (ax | ay) x 2
+  uint8_t* abuf = cbuf + size_t(cpm) * 16;                            // ax x 2
   const size_t abytes = (size_t(apm) * 2 + 127) & ~size_t(127);
-  uint8_t* ring = abuf + 4 * abytes;
+  uint8_t* ring = abuf + 2 * abytes;
   uint8_t* sLp = ring + NS * STAGE;
   uint8_t* sRp = sLp + maxW;
   const int tid = threadIdx.x;
-  int* err = b.err;
-  int* tickets = err + kTicketBase + G;
-  const int total = b.rows_prefix[b.n];
   if (tid == 0) {
     for (int i = 0; i < 4 + NS; ++i) mbar_init(&bars[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_ticket[0] = atomicAdd(tickets, 1);
   }
   {
     int16_t* t16 = reinterpret_cast<int16_t*>(tabp);
@@ -415,27 +350,33 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
   }
   __syncthreads();
   const void* tab = static_cast<const void*>(tabp);
-  const int hw = cfg.hw, dmin = cfg.dmin, hh = cfg.hh;
+  const int hw = cfg.hw, dmin = cfg.dmin;
+  const int total = b.rows_prefix[b.n];
+  int* err = b.err;
   const uint64_t* sL = reinterpret_cast<const uint64_t*>(cbuf);       // + lpad below
   const uint64_t* sR = reinterpret_cast<const uint64_t*>(cbuf + size_t(cpm) * 8);
 
-  auto issue_census = [&](int ticket) {               // thread 0
+  auto row_of = [&](int item, int* y) -> const DevPair& {
+    const int pi = find_pair(b.rows_prefix, b.n, item);
+    *y = cfg.hh + (item - b.rows_prefix[pi]);
+    return b.p[pi];
+  };
+  auto issue_census = [&](int item) {                 // thread 0
     int y;
-    const DevPair& P = b.p[ticket_row(b, ticket, hh, &y)];
+    const DevPair& P = row_of(item, &y);
     const uint32_t cb = uint32_t(P.cpitch) * 8;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_expect(&bars[0], 2 * cb);
     bulk_load(cbuf, P.cwL + size_t(y) * P.cpitch, cb, &bars[0]);
     bulk_load(cbuf + size_t(cpm) * 8, P.cwR + size_t(y) * P.cpitch, cb, &bars[0]);
   };
-  auto issue_coef = [&](int ticket, int buf) {        // thread 0: the ax and ay rows
+  auto issue_ax = [&](int item, int buf) {            // thread 0
     int y;
-    const DevPair& P = b.p[ticket_row(b, ticket, hh, &y)];
+    const DevPair& P = row_of(item, &y);
     const uint32_t ab = uint32_t(P.apitch) * 2;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect(&bars[1 + buf], 2 * ab);
-    bulk_load(abuf + (2 * buf) * abytes, P.ax + size_t(y) * P.apitch, ab, &bars[1 + buf]);
-    bulk_load(abuf + (2 * buf + 1) * abytes, P.ay + size_t(y) * P.apitch, ab, &bars[1 + buf]);
+    mbar_expect(&bars[1 + buf], ab);
+    bulk_load(abuf + buf * abytes, P.ax + size_t(y) * P.apitch, ab, &bars[1 + buf]);
   };
 
   uint32_t phase = 0;                                 // parity bit per barrier
@@ -443,24 +384,20 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
     mbar_wait(&bars[i], (phase >> i) & 1u, err);
     phase ^= 1u << i;
   };
-  int cur = s_ticket[0];
-  if (tid == 0 && cur < total) { issue_census(cur); issue_coef(cur, 0); }
-  for (int it = 0; cur < total; ++it) {
+  if (tid == 0 && int(blockIdx.x) < total) { issue_census(blockIdx.x); issue_ax(blockIdx.x, 0); }
+  int it = 0;
+  for (int item = blockIdx.x; item < total; item += gridDim.x, ++it) {
     const int buf = it & 1;
-    if (tid == 0) {                                   // the next row, taken now so its
-      const int nxt = atomicAdd(tickets, 1);          // coefficients load during this one
-      s_ticket[(it + 1) & 1] = nxt;
-      if (nxt < total) issue_coef(nxt, buf ^ 1);
-    }
+    const int next = item + int(gridDim.x);
+    if (tid == 0 && next < total) issue_ax(next, buf ^ 1);
     int y;
-    const DevPair& P = b.p[ticket_row(b, cur, hh, &y)];
+    const DevPair& P = row_of(item, &y);
     const int W = P.W;
     const size_t row = size_t(y) * W;
     wait_bar(0);
     wait_bar(1 + buf);
     const uint64_t* sLx = sL + P.lpad;
-    const uint16_t* sax = reinterpret_cast<const uint16_t*>(abuf + (2 * buf) * abytes) + P.lpad;
-    const uint16_t* say = reinterpret_cast<const uint16_t*>(abuf + (2 * buf + 1) * abytes);
+    const uint16_t* sax = reinterpret_cast<const uint16_t*>(abuf + buf * abytes) + P.lpad;
     if (!PACKED) {
       for (int i = tid; i < W; i += blockDim.x) { sLp[i] = P.L[row + i]; sRp[i] = P.R[row + i]; }
       __syncthreads();
@@ -532,12 +469,10 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
         out[x * XS] = pack2(f0, f1);
       }
     }
-    // backward + vertical forward; the census buffer is free now, so the next row's
-    // words start loading
+    // backward; the census buffer is free now, so the next row's words start loading
     fence_proxy_async();                              // our stores before the async reads
     __syncthreads();
-    const int nxt = s_ticket[(it + 1) & 1];
-    if (tid == 0 && nxt < total) issue_census(nxt);
+    if (tid == 0 && next < total) issue_census(next);
     const int xlo_cta = hw + dmin;
     const int jmax = (W - 2) / CH, jmin = xlo_cta / CH;
     auto issue_chunk = [&](int j, int slot) {
@@ -549,41 +484,24 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
     };
     if (tid == 0)
       for (int q = 0; q < NS && jmax - q >= jmin; ++q) issue_chunk(jmax - q, q);
-    // V(y - 1) at this thread's disparity pair; row hh - 1 is all zero
-    const bool has_prev = y > hh;
-    const uint32_t* vprev =
-        reinterpret_cast<const uint32_t*>(P.vol + (row - (has_prev ? W : 0)) * DP) + tid;
-    const int* prev_done = P.vprog + (has_prev ? y - 1 : y);
-    int* my_done = P.vprog + y;
     int32_t g0 = f0, g1 = f1;                         // seed: forward value at W-1
     int slot = 0;
     for (int j = jmax; j >= jmin; --j) {
       wait_bar(4 + slot);
-      if (has_prev) wait_progress(prev_done, jmax - j + 1, err);
       const int xa = j * CH;
       const uint32_t* cb = reinterpret_cast<const uint32_t*>(ring + slot * STAGE) + tid;
       const int xhi = min(W - 2, xa + CH - 1);
       const int xlo = max(xa, xw);
-      if (j == jmax) {                                // column W-1 keeps its forward value
-        const uint32_t vp = has_prev ? __ldcg(vprev + size_t(W - 1) * XS) : 0u;
-        const int32_t a = say[W - 1];
-        out[size_t(W - 1) * XS] = pack2(rf_step(g0, lo16(vp), a), rf_step(g1, hi16(vp), a));
-      }
       if (xhi == xa + CH - 1 && xlo == xa) {          // a full chunk: unrolled
         uint32_t* o = out + xa * XS;
         const uint16_t* a1p = sax + xa + 1;
-        const uint16_t* ayp = say + xa;
-        uint32_t pv[CH];
-#pragma unroll
-        for (int q = 0; q < CH; ++q) pv[q] = has_prev ? __ldcg(vprev + size_t(xa + q) * XS) : 0u;
 #pragma unroll
         for (int q = CH - 1; q >= 0; --q) {
           const uint32_t c = cb[q * XS];
           const int32_t a = a1p[q];
           g0 = rf_step(lo16(c), g0, a);
           g1 = rf_step(hi16(c), g1, a);
-          const int32_t av = ayp[q];
-          o[q * XS] = pack2(rf_step(g0, lo16(pv[q]), av), rf_step(g1, hi16(pv[q]), av));
+          o[q * XS] = pack2(g0, g1);
         }
       } else {
         for (int x = xhi; x >= xlo; --x) {
@@ -591,20 +509,13 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
           const int32_t a = sax[x + 1];
           g0 = rf_step(lo16(c), g0, a);
           g1 = rf_step(hi16(c), g1, a);
-          const uint32_t vp = has_prev ? __ldcg(vprev + size_t(x) * XS) : 0u;
-          const int32_t av = say[x];
-          out[x * XS] = pack2(rf_step(g0, lo16(vp), av), rf_step(g1, hi16(vp), av));
+          out[x * XS] = pack2(g0, g1);
         }
       }
-      __syncthreads();                                // stage consumed, chunk stored
-      if (tid == 0) {
-        __threadfence();
-        st_release_gpu(my_done, jmax - j + 1);        // row y + 1 may read this chunk
-        if (j - NS >= jmin) issue_chunk(j - NS, slot);
-      }
+      __syncthreads();                                // stage consumed by every thread
+      if (tid == 0 && j - NS >= jmin) issue_chunk(j - NS, slot);
       slot = (slot + 1 == NS) ? 0 : slot + 1;
     }
-    cur = nxt;
   }
 }
 
@@ -617,8 +528,8 @@ __device__ __forceinline__ uint32_t pk16(int32_t lo, int32_t hi) {
   return __byte_perm(uint32_t(lo), uint32_t(hi), 0x5410);
 }
 
-// k_cols: vertical backward + top-2 + neighbours over the vertical forward values the
-// row kernel stored.  Vertical passes: core/tools/de_dense.cpp:490-507.  Top-2 semantics: :1276-1292
+// k_cols: vertical forward (in place), vertical backward + top-2 + neighbours.
+// Vertical passes: core/tools/de_dense.cpp:490-507.  Top-2 semantics: :1276-1292
 // (ascending k, strictly greater, ties keep the smaller k), sub-pixel neighbour
 // capture :1276-1285.
 //
@@ -701,7 +612,6 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   uint32_t* gcol = reinterpret_cast<uint32_t*>(P.vol + size_t(colok ? x : xbase) * Dpad +
                                                (live ? k0 : 0));
   const uint16_t* ay = P.ay + (colok ? x : xbase);
-  const size_t ap = P.apitch;                         // ay row pitch
   int32_t st[KT];
 #pragma unroll
   for (int s = 0; s < KT; ++s) st[s] = 0;
@@ -721,32 +631,45 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   // load issued PF rows ahead stays in flight until its row; a guarded tail finishes.
   uint32_t ring[PF][KW] = {};
   int32_t aring[PF] = {};
-  // ---- rows yin..H-1 have zero input: V(y) = step(0, V(y - 1)) from V(yin - 1), the
-  // last row the row kernel stores; held in registers for the backward pass ----------
-  if (yin - 1 < hh) return;                           // no row with candidates
-  uint32_t vb[4][KW];                                 // V(yin + r), r < H - yin = hh <= 4
-  {
+  const int ylast = clampi(yin - 1, 0, H - 1);        // last row with input
+  // ---- vertical forward, rows hh..H-1, results stored in place --------------------
+  auto fwd = [&](int y, int j) {
     uint32_t c[KW];
-    fetch(yin - 1, c);
 #pragma unroll
-    for (int i = 0; i < KW; ++i) {
-      st[2 * i] = sx16(c[i]);
-      st[2 * i + 1] = hx16(c[i]);
+    for (int i = 0; i < KW; ++i) c[i] = (y < yin) ? ring[j][i] : 0u;
+    const int32_t a = aring[j];
+    const int yn = y + PF;
+    fetch(min(yn, ylast), ring[j]);
+    aring[j] = ay[size_t(min(yn, H - 1)) * W];
+    step(c, a);
+    if (live) {
+      uint32_t o[KW];
+      pack_state(o);
+      vstore<KW>(gcol + size_t(y) * grs, o);
     }
-    const uint32_t zero[KW] = {};
+  };
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-      if (yin + r < H) {
-        step(zero, ay[size_t(yin + r) * ap]);
-        pack_state(vb[r]);
-      }
+  for (int j = 0; j < PF; ++j) {
+    fetch(min(hh + j, ylast), ring[j]);
+    aring[j] = ay[size_t(min(hh + j, H - 1)) * W];
   }
-  // ---- vertical backward from H-1 (its value is the forward one) + top-2 ----------
-  // Rows yin..H-2 carry no candidates: steps on the register-held values.
+  int y0 = hh;
+  for (; y0 + PF <= H; y0 += PF) {
 #pragma unroll
-  for (int r = 3; r >= 0; --r)
-    if (yin + r <= H - 2) step(vb[r], ay[size_t(yin + r + 1) * ap]);
-  int ys = yin - 1;
+    for (int j = 0; j < PF; ++j) fwd(y0 + j, j);
+  }
+#pragma unroll
+  for (int j = 0; j < PF; ++j)
+    if (y0 + j < H) fwd(y0 + j, j);
+  // ---- vertical backward from H-1 (its value is the forward one) + top-2 ----------
+  // Rows yin..H-2 carry no candidates: plain steps with direct loads.
+  int ys = H - 2;
+  for (; ys >= yin && ys >= hh; --ys) {
+    uint32_t c[KW];
+    fetch(ys, c);
+    step(c, ay[size_t(ys + 1) * W]);
+  }
+  if (ys < hh) return;
   int16_t* rowbufs[kRB];
 #pragma unroll
   for (int i = 0; i < kRB; ++i) rowbufs[i] = &sbuf[wib][i][gbase * KT];
@@ -762,7 +685,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
       const int32_t a = aring[j];
       const int yn = y - PF;
       fetch(max(yn, 0), ring[j]);
-      aring[j] = ay[size_t(max(yn + 1, 0)) * ap];
+      aring[j] = ay[size_t(max(yn + 1, 0)) * W];
       step(c, a);
       pk0 = 0;
       pk1 = 0;                                        // key 0 never displaces a candidate
@@ -833,7 +756,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
       fetch(max(ys - j, 0), ring[j]);
-      aring[j] = ay[size_t(max(ys - j + 1, 0)) * ap];  // coefficient at y + 1
+      aring[j] = ay[size_t(max(ys - j + 1, 0)) * W];   // coefficient at y + 1
     }
     int yb = ys;
     static_assert(PF % kRB == 0, "rows are taken kRB at a time");
@@ -1245,7 +1168,7 @@ size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   }
   size_t s = size_t(TS) * 64 * 2;
   s += size_t(cpm) * 16;
-  s += 4 * ((size_t(apm) * 2 + 127) & ~size_t(127));    // ax and ay rows, double-buffered
+  s += 2 * ((size_t(apm) * 2 + 127) & ~size_t(127));
   s += size_t(3) * (2048 / (64 * G)) * (64 * G) * 2;
   if (!packed) s += size_t(maxW) * 2;
   return (s + 15) & ~size_t(15);
@@ -1308,33 +1231,6 @@ cudaError_t launch_rows_g(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   return TS == 16 ? launch_rows_t<false, 16, G>(cfg, b, s) : launch_rows_t<false, 256, G>(cfg, b, s);
 }
 
-// The row kernel's ticket order (Batch::seg_*): row-major over the pairs, pairs
-// sorted by row count (most first), so at row r the active pairs are a prefix of the
-// order and each run of equal activity is one segment.
-void order_rows(Batch* b) {
-  int n[kMaxBatch], m = 0;
-  for (int i = 0; i < b->n; ++i) {
-    const int rows = b->rows_prefix[i + 1] - b->rows_prefix[i];
-    if (rows > 0) b->ord_pair[m++] = i;
-  }
-  std::stable_sort(b->ord_pair, b->ord_pair + m, [&](int a, int c) {
-    return b->rows_prefix[a + 1] - b->rows_prefix[a] > b->rows_prefix[c + 1] - b->rows_prefix[c];
-  });
-  for (int k = 0; k < m; ++k) n[k] = b->rows_prefix[b->ord_pair[k] + 1] - b->rows_prefix[b->ord_pair[k]];
-  int s = 0, t = 0, prev = 0;
-  for (int c = m; c >= 1; --c) {                      // c pairs active while r < n[c - 1]
-    if (n[c - 1] <= prev) continue;
-    b->seg_t[s] = t;
-    b->seg_r[s] = prev;
-    b->seg_c[s] = c;
-    t += (n[c - 1] - prev) * c;
-    prev = n[c - 1];
-    ++s;
-  }
-  b->seg_t[s] = t;
-  b->seg_n = s;
-}
-
 // One launch per disparity group present in the batch (Dpad = 64 G).
 cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   if (b.rows_prefix[b.n] == 0) return cudaSuccess;
@@ -1351,7 +1247,6 @@ cudaError_t launch_rows(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
       ++sub.n;
     }
     if (sub.n == 0 || sub.rows_prefix[sub.n] == 0) continue;
-    order_rows(&sub);
     cudaError_t e;
     switch (G) {
       case 1: e = launch_rows_g<1>(cfg, sub, s); break;

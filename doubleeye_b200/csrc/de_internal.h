@@ -27,11 +27,8 @@ struct DevPair {
   uint64_t* cwL;       // census word | pixel << 56 (7x7) or census only (wider windows);
   uint64_t* cwR;       //   element (y, x) at [y*cpitch + lpad + x] (left), [y*cpitch + x]
   uint16_t* ax;        // Q15 filter coefficients of L, x direction, [y*apitch + lpad + x]
-  uint16_t* ay;        // ... y direction, [y*apitch + x]
-  int16_t* vol;        // [H][W][Dpad] int16 (Q14): horizontally filtered, then the
-                       //   vertical forward pass applied row by row (the row kernel)
-  int* vprog;          // per image row: backward chunks whose vertical forward values are
-                       //   stored (the next row's row kernel waits on it); zeroed by census
+  uint16_t* ay;        // ... y direction, [y*W + x]
+  int16_t* vol;        // [H][W][Dpad] filtered cost, int16 (Q14)
   uint32_t* key0;      // packed top-2 keys, (v + 32768) << 8 | (255 - k); 0 = empty
   uint32_t* key1;
   uint32_t* nb;        // winner's neighbour costs, lo16 = k*-1, hi16 = k*+1 (-32768 none)
@@ -65,24 +62,10 @@ struct DevCfg {
   uint16_t rf[256];    // Q15 filter coefficient per byte difference
 };
 
-// Head of every dense workspace (kStatusBytes): the status word at [0], then the row
-// kernel's ticket counters, one per disparity group (Dpad = 64 G) at [kTicketBase + G],
-// zeroed by the census kernel.
-constexpr int kTicketBase = 16;
-
 struct Batch {
   int n;
   int maxDpad;
   int* err;            // device status word (bounded waits that ran out set it)
-  // Row-kernel ticket order: tickets run over image rows r = y - hh, row-major across
-  // the pairs (every pair's row 0, then every pair's row 1, ...), so the rows in flight
-  // are spread over all pairs and a pair's consecutive rows start one after another.
-  // Segment s covers tickets [seg_t[s], seg_t[s + 1]): rows seg_r[s] + (t - seg_t[s]) /
-  // seg_c[s] of the seg_c[s] pairs ord_pair[0 .. seg_c[s]) (pairs sorted by row count,
-  // most first).
-  int seg_n;
-  int seg_t[kMaxBatch + 1], seg_r[kMaxBatch], seg_c[kMaxBatch];
-  int ord_pair[kMaxBatch];
   int rows_prefix[kMaxBatch + 1];   // row-kernel work items (rows in [hh, H-hh))
   int cols_prefix[kMaxBatch + 1];   // column-kernel work items (cols with candidates)
   int solve_prefix[kMaxBatch + 1];  // solve work items (all rows)

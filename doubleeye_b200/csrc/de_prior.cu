@@ -168,7 +168,7 @@ __global__ void k_prior_cols(DevCfg cfg, DevPair P, const int* __restrict__ box,
   const size_t st = size_t(W) * Dpad;
   int32_t f = col[size_t(r.ylo) * st];
   for (int y = r.ylo + 1; y < r.yhi; ++y) {
-    f = rf(col[size_t(y) * st], f, P.ay[size_t(y) * P.apitch + x]);
+    f = rf(col[size_t(y) * st], f, P.ay[size_t(y) * W + x]);
     col[size_t(y) * st] = int16_t(f);
   }
   const int iy0 = max(r.ylo, r.pylo), iy1 = min(r.yhi, r.pyhi + 1);
@@ -184,7 +184,7 @@ __global__ void k_prior_cols(DevCfg cfg, DevPair P, const int* __restrict__ box,
   };
   insert(r.yhi - 1, f);                                  // the last row: forward value
   for (int y = r.yhi - 2; y >= r.ylo; --y) {
-    f = rf(col[size_t(y) * st], f, P.ay[size_t(y + 1) * P.apitch + x]);
+    f = rf(col[size_t(y) * st], f, P.ay[size_t(y + 1) * W + x]);
     insert(y, f);
   }
 }

@@ -161,6 +161,19 @@ SIGNATURES = {
     "de_server_destroy": (C.c_int, [vp]),
     "de_dedd_encode_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, vp, vp]),
     "de_server_stream_prior": (C.c_int, [vp, C.c_int, C.c_int]),
+    "de_match_masda_prior_dev": (C.c_int, [vp, vp, C.c_int, vp, vp, vp, C.c_int, vp,
+                                           C.POINTER(DeMatchCfg), vp, vp, C.c_int, vp, vp,
+                                           vp, C.c_size_t, vp]),
+    "de_ctx_census": (C.c_int, [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]),
+    "de_ctx_census_at": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, C.c_int, C.c_int, C.c_int,
+                                   vp, vp]),
+    "de_ctx_detect_fast": (C.c_int, [vp, vp, C.c_int, C.c_int, C.POINTER(DeDetCfg), vp,
+                                     C.c_int, C.POINTER(C.c_int)]),
+    "de_ctx_match_masda": (C.c_int, [vp, vp, vp, C.c_int, vp, vp, C.c_int,
+                                     C.POINTER(DeMatchCfg), vp, vp, C.c_int,
+                                     C.POINTER(C.c_int), vp]),
+    "de_ctx_solve": (C.c_int, [vp, C.POINTER(DeCfg), C.c_int, C.c_int, vp, vp, vp, vp, vp, vp,
+                               vp]),
     "de_prior_fill_workspace_bytes": (C.c_size_t, [C.c_int, C.c_int]),
     "de_prior_fill_dev": (C.c_int, [vp, vp, C.c_int, C.c_int, vp, C.c_size_t, vp]),
 }

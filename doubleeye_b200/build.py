@@ -94,8 +94,33 @@ def build_probe(force: bool = False, verbose: bool = False) -> str:
     return PROBE_LIB
 
 
+CPP_SRC = os.path.join(PKG, "cpp", "doubleeye_shim.cpp")
+CPP_LIB = os.path.join(OUT_DIR, "libdoubleeye_cpp.a")   # the C++14 surface over the C ABI
+
+
+def build_cpp(force: bool = False, verbose: bool = False) -> str:
+    """libdoubleeye_cpp.a: the reference's C++ call surface (include/doubleeye/*.hpp)
+    over the C ABI; callers link it with libdoubleeye_b200.so."""
+    inc = os.path.join(os.path.dirname(PKG), "include")
+    deps = [CPP_SRC] + [os.path.join(inc, "doubleeye", f) for f in os.listdir(os.path.join(inc, "doubleeye"))]
+    deps.append(os.path.join(inc, "doubleeye_b200.h"))
+    if not force and os.path.exists(CPP_LIB) and \
+            os.path.getmtime(CPP_LIB) >= max(os.path.getmtime(d) for d in deps):
+        return CPP_LIB
+    obj = CPP_LIB[:-2] + ".o"
+    cmd = [shutil.which("g++") or "g++", "-O2", "-std=c++14", "-fPIC", "-Wall", "-I", inc,
+           "-c", CPP_SRC, "-o", obj]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    subprocess.run(["ar", "rcs", CPP_LIB + ".tmp", obj], check=True)
+    os.replace(CPP_LIB + ".tmp", CPP_LIB)
+    return CPP_LIB
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     build_probe(force, verbose)
+    build_cpp(force, verbose)
     if not force and not stale():
         build_cli(False, verbose)
         return LIB

@@ -487,7 +487,9 @@ int de_solve_dev(const de_cfg* cfg, int W, int H, const float* cs, const int* cd
                  const int* cn, const int16_t* cnb, float* disp, float* margin,
                  float* lrc2, void* stream) {
   int rc = check_cfg(cfg);
-  if (rc || (rc = check_dims(W, H))) return rc;
+  if (rc) return rc;
+  if (W < 1 || H < 1 || W > de::kMaxW || H > de::kMaxH)   // any row count, one row too
+    return fail(DE_ERR_ARG, "candidates %dx%d outside 1..%d x 1..%d", W, H, de::kMaxW, de::kMaxH);
   if (!cs || !cd || !cn || !disp) return fail(DE_ERR_ARG, "NULL buffer");
   de_cfg c2 = *cfg;
   c2.lrc = 0;
@@ -983,6 +985,205 @@ int de_ctx_dense(de_ctx* c, const uint8_t* L, const uint8_t* R, int W, int H, fl
   p.L = L; p.R = R; p.W = W; p.H = H; p.dmax = 0;
   p.disp = disp; p.margin = margin; p.conf = conf; p.cand = cand;
   return de_ctx_dense_batch(c, &p, 1);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------
+// Host-pointer forms of the stage and sparse entry points: inputs copied up into the
+// context's I/O block, the device entry point run on the context's stream, outputs
+// copied back; each call has finished when it returns.
+namespace {
+
+struct Carve {                                       // consecutive 256-byte aligned slices
+  size_t end = 0;
+  size_t take(size_t n) {
+    const size_t o = end;
+    end = align_up(end + std::max<size_t>(n, 1));
+    return o;
+  }
+};
+
+int ctx_io(de_ctx* c, size_t io_bytes, size_t ws_bytes) {
+  DE_CUDA(cudaSetDevice(c->device));
+  if (int rc = grow_dev(&c->dio, &c->dio_cap, io_bytes)) return rc;
+  return grow_dev(&c->dws, &c->dws_cap, std::max<size_t>(ws_bytes, 256));
+}
+
+int ctx_up(de_ctx* c, size_t off, const void* src, size_t n) {
+  if (!n) return DE_OK;
+  DE_CUDA(cudaMemcpyAsync(static_cast<uint8_t*>(c->dio) + off, src, n, cudaMemcpyHostToDevice,
+                          c->stream));
+  return DE_OK;
+}
+
+int ctx_down(de_ctx* c, void* dst, size_t off, size_t n) {
+  if (!n || !dst) return DE_OK;
+  DE_CUDA(cudaMemcpyAsync(dst, static_cast<uint8_t*>(c->dio) + off, n, cudaMemcpyDeviceToHost,
+                          c->stream));
+  return DE_OK;
+}
+
+template <typename T = void>
+T* dptr(de_ctx* c, size_t off) {
+  return reinterpret_cast<T*>(static_cast<uint8_t*>(c->dio) + off);
+}
+
+}  // namespace
+
+extern "C" {
+
+int de_ctx_census(de_ctx* c, const uint8_t* img, int W, int H, int hw, int hh,
+                  uint64_t* bits) {
+  if (!c || !img || !bits) return fail(DE_ERR_ARG, "NULL argument");
+  if (int rc = check_dims(W, H)) return rc;
+  const size_t WH = size_t(W) * H;
+  Carve k;
+  const size_t oi = k.take(WH), ob = k.take(WH * 8), ob2 = k.take(WH * 8);
+  const size_t oax = k.take(WH * 2), oay = k.take(WH * 2);
+  if (int rc = ctx_io(c, k.end, 0)) return rc;
+  de_cfg cfg = c->cfg;
+  cfg.census_hw = hw;
+  cfg.census_hh = hh;
+  int rc = ctx_up(c, oi, img, WH);
+  if (!rc) rc = de_census_dev(&cfg, dptr<uint8_t>(c, oi), dptr<uint8_t>(c, oi), W, H,
+                              dptr<uint64_t>(c, ob), dptr<uint64_t>(c, ob2),
+                              dptr<uint16_t>(c, oax), dptr<uint16_t>(c, oay), c->stream);
+  if (!rc) rc = ctx_down(c, bits, ob, WH * 8);
+  if (rc) return rc;
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  return DE_OK;
+}
+
+int de_ctx_census_at(de_ctx* c, const uint8_t* img, int W, int H, const de_keypoint* kp,
+                     int n, int hw, int hh, uint64_t* desc, uint8_t* ok) {
+  if (!c || !img || n < 0 || (n > 0 && (!kp || !desc))) return fail(DE_ERR_ARG, "bad argument");
+  if (W < 1 || H < 1) return fail(DE_ERR_ARG, "image %dx%d", W, H);
+  if (n == 0) return DE_OK;
+  const size_t WH = size_t(W) * H;
+  Carve k;
+  const size_t oi = k.take(WH), ok_ = k.take(sizeof(de_keypoint) * n);
+  const size_t od = k.take(8 * size_t(n)), oo = k.take(size_t(n));
+  if (int rc = ctx_io(c, k.end, 0)) return rc;
+  int rc = ctx_up(c, oi, img, WH);
+  if (!rc) rc = ctx_up(c, ok_, kp, sizeof(de_keypoint) * n);
+  if (!rc) rc = de_census_at_dev(dptr<uint8_t>(c, oi), W, H, dptr<de_keypoint>(c, ok_), n,
+                                 nullptr, hw, hh, dptr<uint64_t>(c, od), dptr<uint8_t>(c, oo),
+                                 c->stream);
+  if (!rc) rc = ctx_down(c, desc, od, 8 * size_t(n));
+  if (!rc) rc = ctx_down(c, ok, oo, size_t(n));
+  if (rc) return rc;
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  return DE_OK;
+}
+
+int de_ctx_detect_fast(de_ctx* c, const uint8_t* img, int W, int H, const de_det_cfg* cfg,
+                       de_keypoint* out, int cap, int* n) {
+  if (!c || !img || !cfg || !n || cap < 0 || (cap > 0 && !out))
+    return fail(DE_ERR_ARG, "bad argument");
+  size_t ws = 0;
+  if (int rc = de_detect_workspace_bytes(W, H, cfg, &ws)) return rc;
+  const size_t WH = size_t(W) * H;
+  Carve k;
+  const size_t oi = k.take(WH), oo = k.take(sizeof(de_keypoint) * size_t(std::max(cap, 1)));
+  const size_t on = k.take(sizeof(int));
+  if (int rc = ctx_io(c, k.end, ws)) return rc;
+  int rc = ctx_up(c, oi, img, WH);
+  if (!rc) rc = de_detect_fast_dev(dptr<uint8_t>(c, oi), W, H, cfg, dptr<de_keypoint>(c, oo),
+                                   cap, dptr<int>(c, on), c->dws, c->dws_cap, c->stream);
+  if (!rc) rc = ctx_down(c, n, on, sizeof(int));
+  if (rc) return rc;
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  if (*n < 0) return fail(DE_ERR_UNSUPPORTED, "keypoint suppression exceeded its work bound");
+  const int got = std::min(*n, cap);
+  if (got > 0) {
+    DE_CUDA(cudaMemcpy(out, dptr(c, oo), sizeof(de_keypoint) * size_t(got),
+                       cudaMemcpyDeviceToHost));
+  }
+  return DE_OK;
+}
+
+int de_ctx_match_masda(de_ctx* c, const de_keypoint* kl, const uint64_t* dl, int nl,
+                       const de_keypoint* kr, const uint64_t* dr, int nr,
+                       const de_match_cfg* cfg, const de_match_prior* prior, de_match* out,
+                       int cap, int* n_out, de_match_stats* stats) {
+  if (!c || !cfg || !n_out || nl < 0 || nr < 0 || cap < 0 || (cap > 0 && !out))
+    return fail(DE_ERR_ARG, "bad argument");
+  size_t ws = 0;
+  if (int rc = de_match_workspace_bytes(nl, nr, cfg, &ws)) return rc;
+  Carve k;
+  const size_t okl = k.take(sizeof(de_keypoint) * nl), odl = k.take(8 * size_t(nl));
+  const size_t okr = k.take(sizeof(de_keypoint) * nr), odr = k.take(8 * size_t(nr));
+  const size_t oout = k.take(sizeof(de_match) * size_t(std::max(cap, 1)));
+  const size_t on = k.take(sizeof(int)), ost = k.take(sizeof(de_match_stats));
+  const size_t pn = 4 * size_t(nl);
+  const size_t pcd = k.take(pn), pcs = k.take(pn), psd = k.take(pn), pss = k.take(pn);
+  if (int rc = ctx_io(c, k.end, ws)) return rc;
+  int rc = ctx_up(c, okl, kl, sizeof(de_keypoint) * nl);
+  if (!rc) rc = ctx_up(c, odl, dl, 8 * size_t(nl));
+  if (!rc) rc = ctx_up(c, okr, kr, sizeof(de_keypoint) * nr);
+  if (!rc) rc = ctx_up(c, odr, dr, 8 * size_t(nr));
+  de_match_prior dp{};
+  if (!rc && prior) {
+    dp.w_coarse = prior->w_coarse;
+    dp.w_smooth = prior->w_smooth;
+    if (prior->coarse_sd) {
+      if (!prior->coarse_d) return fail(DE_ERR_ARG, "coarse prior sigma without disparities");
+      rc = ctx_up(c, pcd, prior->coarse_d, pn);
+      if (!rc) rc = ctx_up(c, pcs, prior->coarse_sd, pn);
+      dp.coarse_d = dptr<float>(c, pcd);
+      dp.coarse_sd = dptr<float>(c, pcs);
+    }
+    if (!rc && prior->smooth_sd) {
+      if (!prior->smooth_d) return fail(DE_ERR_ARG, "smooth prior sigma without disparities");
+      rc = ctx_up(c, psd, prior->smooth_d, pn);
+      if (!rc) rc = ctx_up(c, pss, prior->smooth_sd, pn);
+      dp.smooth_d = dptr<float>(c, psd);
+      dp.smooth_sd = dptr<float>(c, pss);
+    }
+  }
+  if (!rc) rc = de_match_masda_prior_dev(dptr<de_keypoint>(c, okl), dptr<uint64_t>(c, odl), nl,
+                                         nullptr, dptr<de_keypoint>(c, okr),
+                                         dptr<uint64_t>(c, odr), nr, nullptr, cfg,
+                                         prior ? &dp : nullptr, dptr<de_match>(c, oout), cap,
+                                         dptr<int>(c, on), dptr<de_match_stats>(c, ost), c->dws,
+                                         c->dws_cap, c->stream);
+  if (!rc) rc = ctx_down(c, n_out, on, sizeof(int));
+  if (!rc) rc = ctx_down(c, stats, ost, sizeof(de_match_stats));
+  if (rc) return rc;
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  const int got = std::min(*n_out, cap);
+  if (got > 0) {
+    DE_CUDA(cudaMemcpy(out, dptr(c, oout), sizeof(de_match) * size_t(got),
+                       cudaMemcpyDeviceToHost));
+  }
+  return DE_OK;
+}
+
+int de_ctx_solve(de_ctx* c, const de_cfg* cfg, int W, int H, const float* cs, const int* cd,
+                 const int* cn, const int16_t* cnb, float* disp, float* margin, float* lrc2) {
+  if (!c || !cs || !cd || !cn || !disp) return fail(DE_ERR_ARG, "NULL buffer");
+  if (W < 1 || H < 1) return fail(DE_ERR_ARG, "candidates %dx%d", W, H);
+  const size_t WH = size_t(W) * H;
+  Carve k;
+  const size_t ocs = k.take(WH * 8), ocd = k.take(WH * 8), ocn = k.take(WH * 4);
+  const size_t onb = k.take(WH * 4), od = k.take(WH * 4), om = k.take(WH * 4);
+  const size_t ol = k.take(WH * 4);
+  if (int rc = ctx_io(c, k.end, 0)) return rc;
+  int rc = ctx_up(c, ocs, cs, WH * 8);
+  if (!rc) rc = ctx_up(c, ocd, cd, WH * 8);
+  if (!rc) rc = ctx_up(c, ocn, cn, WH * 4);
+  if (!rc && cnb) rc = ctx_up(c, onb, cnb, WH * 4);
+  if (!rc) rc = de_solve_dev(cfg, W, H, dptr<float>(c, ocs), dptr<int>(c, ocd),
+                             dptr<int>(c, ocn), cnb ? dptr<int16_t>(c, onb) : nullptr,
+                             dptr<float>(c, od), dptr<float>(c, om),
+                             lrc2 ? dptr<float>(c, ol) : nullptr, c->stream);
+  if (!rc) rc = ctx_down(c, disp, od, WH * 4);
+  if (!rc) rc = ctx_down(c, margin, om, WH * 4);
+  if (!rc) rc = ctx_down(c, lrc2, ol, WH * 4);
+  if (rc) return rc;
+  DE_CUDA(cudaStreamSynchronize(c->stream));
+  return DE_OK;
 }
 
 }  // extern "C"

@@ -552,6 +552,7 @@ struct MatchArgs {
   float max_dy, min_disp, max_disp, sigma_y, w_y, damping, lambda, gamma, eps;
   int maxc, iters, census_bits;
   int smem_bytes;         // dynamic shared memory of the launch
+  de_match_prior prior;   // soft disparity priors per left keypoint (arrays may be null)
 };
 
 __device__ __forceinline__ uint32_t ord_f32(float v) {   // order-preserving bits
@@ -559,12 +560,32 @@ __device__ __forceinline__ uint32_t ord_f32(float v) {   // order-preserving bit
   return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
+// pair_score, core/src/match.cpp:298-332: descriptor agreement minus the y-residual
+// penalty, minus each soft disparity prior's penalty where left keypoint i has one
+// (sigma > 0), in the reference's order of operations.
 __device__ __forceinline__ float pair_score(const de_keypoint& l, const de_keypoint& r,
-                                            uint64_t dl, uint64_t dr, const MatchArgs& a) {
+                                            uint64_t dl, uint64_t dr, const MatchArgs& a,
+                                            int i) {
   const float half = 0.5f * float(a.census_bits);
   const float desc = (half - float(__popcll(dl ^ dr))) / half;
   const float dy = (l.y - r.y) / (a.sigma_y > 0 ? a.sigma_y : 1.f);
-  return desc - a.w_y * dy * dy;
+  float score = desc - a.w_y * dy * dy;
+  const de_match_prior& p = a.prior;
+  if (p.coarse_sd) {
+    const float sd = p.coarse_sd[i];
+    if (sd > 0.f) {
+      const float e = ((l.x - r.x) - p.coarse_d[i]) / sd;
+      score -= p.w_coarse * e * e;
+    }
+  }
+  if (p.smooth_sd) {
+    const float sd = p.smooth_sd[i];
+    if (sd > 0.f) {
+      const float e = ((l.x - r.x) - p.smooth_d[i]) / sd;
+      score -= p.w_smooth * e * e;
+    }
+  }
+  return score;
 }
 
 // Priority of the greedy completion: belief desc, score desc, edge index asc.
@@ -672,7 +693,7 @@ __global__ void __launch_bounds__(1024, 1) k_match(MatchArgs a, MatchWs m) {
         const float d = l.x - r.x;
         if (d < a.min_disp || d > a.max_disp) continue;
         sj[k] = j;
-        ss[k] = pair_score(l, r, dli, a.dr[j], a);
+        ss[k] = pair_score(l, r, dli, a.dr[j], a, i);
         ++k;
       }
     } else {                  // best maxc by score, in score order (ties: band order)
@@ -681,14 +702,14 @@ __global__ void __launch_bounds__(1024, 1) k_match(MatchArgs a, MatchWs m) {
         const de_keypoint r = a.kr[j];
         const float d = l.x - r.x;
         if (d < a.min_disp || d > a.max_disp) continue;
-        const float s = pair_score(l, r, dli, a.dr[j], a);
+        const float s = pair_score(l, r, dli, a.dr[j], a, i);
         int rank = 0;
         for (int q = lo; q < hi && rank < maxc; ++q) {
           const int jq = int(keys[q] & 0xffffffffu);
           const de_keypoint rq = a.kr[jq];
           const float dq = l.x - rq.x;
           if (dq < a.min_disp || dq > a.max_disp) continue;
-          const float sq = pair_score(l, rq, dli, a.dr[jq], a);
+          const float sq = pair_score(l, rq, dli, a.dr[jq], a, i);
           rank += (sq > s || (sq == s && q < p)) ? 1 : 0;
         }
         if (rank < maxc) {
@@ -1110,8 +1131,9 @@ size_t match_ws_bytes_for(int nl, int nr, const de_match_cfg* c) {
 
 int match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl, const int* nl_dev,
                     const de_keypoint* kr, const uint64_t* dr, int nr, const int* nr_dev,
-                    const de_match_cfg* c, de_match* out, int cap, int* n_out,
-                    de_match_stats* stats, void* ws, size_t bytes, cudaStream_t s) {
+                    const de_match_cfg* c, const de_match_prior* prior, de_match* out,
+                    int cap, int* n_out, de_match_stats* stats, void* ws, size_t bytes,
+                    cudaStream_t s) {
   if (int rc = check_match_cfg(c)) return rc;
   if (nl < 0 || nr < 0 || nl > (1 << 20) || nr > kSortMax)
     return set_error(DE_ERR_ARG, "keypoint counts %d/%d outside 0..%d / 0..%d", nl, nr,
@@ -1131,6 +1153,12 @@ int match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl, const int
   a.sigma_y = c->sigma_y; a.w_y = c->w_y; a.damping = c->damping;
   a.lambda = c->lambda; a.gamma = c->gamma; a.eps = c->converge_eps;
   a.maxc = maxc; a.iters = c->iterations; a.census_bits = c->census_bits;
+  a.prior = de_match_prior{};
+  if (prior) {
+    if ((prior->coarse_sd && !prior->coarse_d) || (prior->smooth_sd && !prior->smooth_d))
+      return set_error(DE_ERR_ARG, "a prior's sigma array is given without its disparities");
+    a.prior = *prior;
+  }
   MatchWs m = carve_match(ws, std::max(nl, 1), std::max(nr, 1), maxc);
   int N = 1;
   while (N < std::max(nr, 1)) N <<= 1;
@@ -1199,8 +1227,18 @@ int de_match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl, const 
                        const de_keypoint* kr, const uint64_t* dr, int nr, const int* nr_dev,
                        const de_match_cfg* cfg, de_match* out, int cap, int* n_out,
                        de_match_stats* stats, void* workspace, size_t bytes, void* stream) {
-  return de::match_masda_dev(kl, dl, nl, nl_dev, kr, dr, nr, nr_dev, cfg, out, cap, n_out,
-                             stats, workspace, bytes, static_cast<cudaStream_t>(stream));
+  return de::match_masda_dev(kl, dl, nl, nl_dev, kr, dr, nr, nr_dev, cfg, nullptr, out, cap,
+                             n_out, stats, workspace, bytes, static_cast<cudaStream_t>(stream));
+}
+
+int de_match_masda_prior_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
+                             const int* nl_dev, const de_keypoint* kr, const uint64_t* dr,
+                             int nr, const int* nr_dev, const de_match_cfg* cfg,
+                             const de_match_prior* prior, de_match* out, int cap, int* n_out,
+                             de_match_stats* stats, void* workspace, size_t bytes,
+                             void* stream) {
+  return de::match_masda_dev(kl, dl, nl, nl_dev, kr, dr, nr, nr_dev, cfg, prior, out, cap,
+                             n_out, stats, workspace, bytes, static_cast<cudaStream_t>(stream));
 }
 
 }  // extern "C"

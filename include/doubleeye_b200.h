@@ -262,6 +262,28 @@ DE_API int de_match_masda_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
                               int cap, int* n_out, de_match_stats* stats, void* workspace,
                               size_t bytes, void* stream);
 
+/* The soft disparity priors of MatchConfig (core/include/doubleeye/match.hpp:157-163:
+ * the coarse DisparityPrior and the per-keypoint SmoothPrior), applied in pair_score
+ * (core/src/match.cpp:298-332), resolved by the caller to one (disparity, sigma) per
+ * LEFT keypoint: s(i,j) -= w * (((xl - xr) - d[i]) / sd[i])^2 where sd[i] > 0, no
+ * term where sd[i] <= 0 (the reference's "no prior here").  Device arrays of nl
+ * floats; a NULL sigma array turns that prior off. */
+typedef struct de_match_prior {
+  const float* coarse_d;
+  const float* coarse_sd;
+  float w_coarse;
+  const float* smooth_d;
+  const float* smooth_sd;
+  float w_smooth;
+} de_match_prior;
+/* de_match_masda_dev with soft disparity priors (prior may be NULL). */
+DE_API int de_match_masda_prior_dev(const de_keypoint* kl, const uint64_t* dl, int nl,
+                                    const int* nl_dev, const de_keypoint* kr,
+                                    const uint64_t* dr, int nr, const int* nr_dev,
+                                    const de_match_cfg* cfg, const de_match_prior* prior,
+                                    de_match* out, int cap, int* n_out, de_match_stats* stats,
+                                    void* workspace, size_t bytes, void* stream);
+
 /* ---- the disparity prior as a per-plane mask (--prior) ------------------------
  * core/tools/de_dense.cpp:797-853,438-483,1166-1297 (run_dense with a prior, the
  * --prior path of :1756-1813).  prior: W x H float32 disparities on the device (a
@@ -440,6 +462,32 @@ DE_API int de_ctx_keypoints(de_ctx* ctx, const uint8_t* L, int W, int H, const d
                             int cap, int* n_out, int* n_detected);
 /* The same for n host pairs in one batched launch. */
 DE_API int de_ctx_dense_batch(de_ctx* ctx, const de_pair* host_pairs, int n);
+
+/* Host-pointer forms of the stage and sparse entry points, for callers without device
+ * memory of their own (the C++ surface in include/doubleeye/ is built on these).
+ * Sizes and limits are those of the device forms above.
+ *   de_ctx_census:      census_transform (core/src/preproc.cpp:110-138) of one image,
+ *                       bits[W*H] (0 outside the (hw, hh) border)
+ *   de_ctx_census_at:   census_at at n keypoints (de_census_at_dev)
+ *   de_ctx_detect_fast: detect_keypoints_fast, *n = keypoints found (at most cap
+ *                       written)
+ *   de_ctx_match_masda: match_masda with optional priors (HOST arrays in prior);
+ *                       *n_out matches (at most cap written), stats may be NULL
+ *   de_ctx_solve:       the row solve over reference-layout candidates (de_solve_dev) */
+DE_API int de_ctx_census(de_ctx* ctx, const uint8_t* img, int W, int H, int hw, int hh,
+                         uint64_t* bits);
+DE_API int de_ctx_census_at(de_ctx* ctx, const uint8_t* img, int W, int H,
+                            const de_keypoint* kp, int n, int hw, int hh, uint64_t* desc,
+                            uint8_t* ok);
+DE_API int de_ctx_detect_fast(de_ctx* ctx, const uint8_t* img, int W, int H,
+                              const de_det_cfg* cfg, de_keypoint* out, int cap, int* n);
+DE_API int de_ctx_match_masda(de_ctx* ctx, const de_keypoint* kl, const uint64_t* dl, int nl,
+                              const de_keypoint* kr, const uint64_t* dr, int nr,
+                              const de_match_cfg* cfg, const de_match_prior* prior,
+                              de_match* out, int cap, int* n_out, de_match_stats* stats);
+DE_API int de_ctx_solve(de_ctx* ctx, const de_cfg* cfg, int W, int H, const float* cs,
+                        const int* cd, const int* cn, const int16_t* cnb, float* disp,
+                        float* margin, float* lrc2);
 
 #ifdef __cplusplus
 }

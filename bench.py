@@ -234,31 +234,50 @@ def max_over_ranks(x: float, ws: int) -> float:
     return mor(x) if ws > 1 else x
 
 
-def cpu_baseline_sample(budget_s: float = 15.0, max_pairs: int = 400) -> dict:
-    """The reference's CPU path on this host's cores: as many pairs as fit in about
-    budget_s seconds (at least 3)."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_sample(reps: int = 5) -> dict:
+    """The reference's CPU path (run_dense, core/tools/de_dense.cpp:738) on this host:
+    one 848x480 D=128 pair, 8 iterations, timed at all host threads and at one thread
+    (the reference's deterministic form), the two interleaved, `reps` times each; the
+    minimum is the reported time and the spread is kept."""
     from oracle import oracle as O
     nthreads = os.cpu_count() or 1
-    pairs = make_pairs(3, 900)
+    pair = make_pairs(1, 900)[0]
     cfg = O.default_cfg(dmax=D, iters=ITERS)
     if O.Reference.available():
         ref = O.Reference()
-        run = lambda p: ref.dense(cfg, p.left, p.right, nthreads=nthreads, want_cand=False)  # noqa
-        kind, cores = "reference", nthreads
+        run = lambda nt: ref.dense(cfg, pair.left, pair.right, nthreads=nt, want_cand=False)  # noqa
+        kind = "reference"
     else:
         orc = O.Oracle()
-        run = lambda p: orc.dense(cfg, p.left, p.right, want_cand=False)  # noqa
-        kind, cores = "port", 1
-    run(pairs[0])                                  # warm caches
-    n, t0 = 0, time.perf_counter()
-    while n < max_pairs and (n < 3 or time.perf_counter() - t0 < budget_s):
-        run(pairs[n % len(pairs)])
-        n += 1
-    dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": "pairs/s", "cores": cores, "kind": kind,
-            "sample": f"{n} pairs 848x480 D=128 iters 8 in {dt:.1f}s, "
-                      f"{'de_dense run_dense' if kind == 'reference' else 'oracle port'}"
-                      f" at {cores} thread(s)"}
+        run = lambda nt: orc.dense(cfg, pair.left, pair.right, want_cand=False)  # noqa
+        kind, nthreads = "port", 1
+    run(nthreads)                                  # warm caches and thread pool
+    t_all, t_one = [], []
+    for _ in range(reps):
+        for nt, acc in ((nthreads, t_all), (1, t_one)):
+            t0 = time.perf_counter()
+            run(nt)
+            acc.append(time.perf_counter() - t0)
+    spread = lambda v: {"min_s": min(v), "median_s": sorted(v)[len(v) // 2],  # noqa: E731
+                        "max_s": max(v)}
+    return {"value": 1.0 / min(t_all), "unit": "pairs/s", "cores": nthreads, "kind": kind,
+            "cpu_model": cpu_model(),
+            "single_thread_pairs_per_s": 1.0 / min(t_one),
+            "all_threads": spread(t_all), "one_thread": spread(t_one),
+            "sample": f"one 848x480 D=128 iters 8 pair, {reps} interleaved repetitions at "
+                      f"{nthreads} and 1 thread(s), minimum reported, "
+                      f"{'reference run_dense' if kind == 'reference' else 'oracle port'}"}
 
 
 def run_reference(args) -> None:
@@ -281,11 +300,15 @@ def run_reference(args) -> None:
     for _ in range(args.warmup):
         for p in pairs:
             run(p)
+    steps = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
+        ts = time.perf_counter()
         for p in pairs:
             run(p)
+        steps.append(time.perf_counter() - ts)
     dt = time.perf_counter() - t0
+    steps.sort()
     n = args.steps * len(pairs)
     v = n / dt
     out = {"metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": ws, "steps": args.steps,
@@ -295,7 +318,10 @@ def run_reference(args) -> None:
            "config": {"workload": "dense 848x480 D=128 iters=8", "W": W, "H": H, "D": D,
                       "iters": ITERS, "pairs_per_step": len(pairs), "parallelism": "cpu"},
            "g_disp_evals_per_s": disp_evals(n) / dt / 1e9,
+           "step_ms": {"min": steps[0] * 1e3, "median": steps[len(steps) // 2] * 1e3,
+                       "max": steps[-1] * 1e3},
            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": kind,
+                            "cpu_model": cpu_model(),
                             "sample": f"{len(pairs)} pairs per step, {what}, "
                                       f"{cores} thread(s)"},
            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0,
@@ -303,32 +329,14 @@ def run_reference(args) -> None:
     print(json.dumps(out), flush=True)
 
 
-def c4_pairs(seed: int = 4):
-    """The uneven batch: 64 slots with sizes drawn uniformly (seed-fixed) from
-    {320x240, 640x480, 848x480, 1280x720, 1920x1080}, D in {64, 128, 256} matched to
-    size; two distinct seeded slanted-plane scenes per size, reused across slots (the
-    generator takes seconds per large scene on the host)."""
-    from doubleeye_b200 import synth
-    shapes = list(synth.BATCH_SHAPES.items())
-    rng = synth.rng_for("batch-draw", synth.BASE_SEED)
-    scenes = {}
-    out = []
-    for i in range(64):
-        (W, H), D = shapes[int(rng.integers(0, len(shapes)))]
-        k = (W, H, i % 2)
-        if k not in scenes:
-            scenes[k] = synth.slanted_planes(W, H, D - 1, seed=seed + len(scenes),
-                                             tag=f"c4:{W}x{H}")
-        out.append((scenes[k], D))
-    return out
-
-
-def run_c4(de, local: int, steps: int, warmup: int) -> dict:
-    """Batched uneven workload: one launch set for all 64 pairs (autotuned launch
-    shapes, CUDA-graph replay) against one launch set per pair."""
+def run_c4(de, local: int, steps: int, warmup: int, c4_set) -> dict:
+    """Batched uneven workload: 64 distinct seeded pairs, sizes drawn uniformly (seed-
+    fixed) from {320x240, 640x480, 848x480, 1280x720, 1920x1080} with D in {64, 128,
+    256} matched to size, in one launch set (autotuned launch shapes, CUDA-graph
+    replay) against one launch set per pair."""
     import torch
-    from doubleeye_b200 import autotune
-    pairs = c4_pairs()
+    from doubleeye_b200 import autotune, synth
+    pairs = [(p, synth.BATCH_SHAPES[(p.left.shape[1], p.left.shape[0])]) for p in c4_set]
     cfg = de.Cfg(iters=ITERS)
     m = de.DenseMatcher(cfg, device=local)
     Ls = [torch.from_numpy(p.left).cuda() for p, _ in pairs]
@@ -360,13 +368,42 @@ def run_c4(de, local: int, steps: int, warmup: int) -> dict:
     for p, D in pairs:
         key = f"{p.left.shape[1]}x{p.left.shape[0]}/D{D}"
         sizes[key] = sizes.get(key, 0) + 1
-    return {"workload": "64 pairs, uneven sizes and D in one launch set", "sizes": sizes,
-            "pairs_per_s": 64 / (ms_batch / 1e3), "graph_pairs_per_s": 64 / (ms_graph / 1e3),
+    hbm_floor_ms = sum(2 * L.numel() + 4 * L.numel() * D + 32 * L.numel()
+                       for L, (_, D) in zip(Ls, pairs)) / (load_peaks()["hbm_gbs"] * 1e6)
+    best = min(ms_batch, ms_graph)
+    return {"workload": "64 distinct pairs, uneven sizes and D in one launch set",
+            "sizes": sizes, "pairs_per_s": 64 / (ms_batch / 1e3),
+            "graph_pairs_per_s": 64 / (ms_graph / 1e3),
             "plain_pairs_per_s": 64 / (ms_plain / 1e3),
-            "batch_over_plain": ms_plain / min(ms_batch, ms_graph),
-            "g_disp_evals_per_s": evals / (min(ms_batch, ms_graph) / 1e3) / 1e9,
-            "ms_per_batch": min(ms_batch, ms_graph), "knobs": knobs,
-            "data": "synthetic, 2 scenes per size reused across the 64 slots"}
+            "batch_over_plain": ms_plain / best,
+            "g_disp_evals_per_s": evals / (best / 1e3) / 1e9,
+            "ms_per_batch": best, "hbm_floor_ms": hbm_floor_ms,
+            "frac_of_hbm_floor": hbm_floor_ms / best, "knobs": knobs,
+            "data": "synthetic, 64 distinct seeded slanted-plane pairs"}
+
+
+def run_py_entry(local: int) -> dict:
+    """The reference's Python entry points on the GPU (float64, as NumPy): the dense
+    edge list of a 450x375 pair at disparities 1..60 (article/dense_masda.py
+    dense_problem) and max-sum over it, 12 iterations (article/masda_stereo.py
+    masda_sparse), the configuration the reference quotes its NumPy time on."""
+    import torch
+    from doubleeye_b200 import dense_masda, masda_stereo, synth
+    p = synth.slanted_planes(450, 375, 59, seed=11, tag="py-entry")
+    out = {}
+    for rep in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ei, ej, se, n = dense_masda.dense_problem(p.left, p.right, 1, 60, device=True)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        assign, hist = masda_stereo.masda_sparse(ei, ej, se, n, n, -0.1, -0.1, 12, 0.4, 1e-9)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out = {"workload": "450x375, disparities 1..60, 12 iterations (float64)",
+               "edges": int(ei.shape[0]), "dense_problem_ms": (t1 - t0) * 1e3,
+               "masda_sparse_ms": (t2 - t1) * 1e3, "total_ms": (t2 - t0) * 1e3}
+    return out
 
 
 def run_c5(de, local: int) -> dict:
@@ -482,6 +519,10 @@ def run_ours(args) -> None:
     B, K, Wm = args.pairs_per_step, args.steps, args.warmup
     from doubleeye_b200.replicas import rank_seed
     pairs = make_pairs(B, rank_seed(rank))
+    c4_set = None
+    if ws == 1 and not args.no_extras:              # 64 distinct pairs, host-generated
+        from doubleeye_b200 import synth
+        c4_set = synth.batch_pairs(64, seed=4, workers=min(16, os.cpu_count() or 1))
     cfg = de.Cfg(dmax=D, iters=ITERS)
     m = de.DenseMatcher(cfg, device=local)
     Ls = [torch.from_numpy(p.left).cuda() for p in pairs]
@@ -491,29 +532,38 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream()
 
     # --- device-timed batched throughput (the headline value) -----------------------
+    # No instrumentation inside the timed region beyond one CUDA event per step (the
+    # spread of step times); the stage split is taken in a separate pass below.
     for _ in range(Wm):
         m.match_into(items)
     torch.cuda.synchronize()
     barrier(ws)
-    lib().de_stage_timing(1)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
     with ClockSampler(local) as clk:
         torch.cuda.synchronize()
         barrier(ws)
-        e0.record(stream)
-        for _ in range(K):
+        ev[0].record(stream)
+        for k in range(K):
             m.match_into(items)
-        e1.record(stream)
+            ev[k + 1].record(stream)
         torch.cuda.synchronize()
-    lib().de_stage_timing(0)
     barrier(ws)
-    ms_local = e0.elapsed_time(e1)
-    stage = (C.c_float * 4)()
-    nl = C.c_int()
-    check(lib().de_stage_times(stage, 4, C.byref(nl)))
+    ms_local = ev[0].elapsed_time(ev[K])
+    step_ms = sorted(ev[k].elapsed_time(ev[k + 1]) for k in range(K))
     ms = max_over_ranks(ms_local, ws)
     total_pairs = ws * B * K
     value = total_pairs / (ms / 1e3)
+
+    # --- stage split (a separate pass with stage events between the kernels) ---------
+    lib().de_stage_timing(1)
+    Ks = min(K, 20)
+    for _ in range(Ks):
+        m.match_into(items)
+    torch.cuda.synchronize()
+    lib().de_stage_timing(0)
+    stage = (C.c_float * 4)()
+    nl = C.c_int()
+    check(lib().de_stage_times(stage, 4, C.byref(nl)))
 
     # --- plain single-pair path, same device timing -------------------------------
     one = [items[0]]
@@ -547,7 +597,7 @@ def run_ours(args) -> None:
     filled = float(np.mean([np.isfinite(r.disp).mean() for r in res]))
 
     # --- roofline of the dominant kernel ------------------------------------------
-    per_launch = {s: stage[i] / max(1, nl.value) for i, s in enumerate(STAGES)}
+    per_launch = {st: stage[i] / max(1, nl.value) for i, st in enumerate(STAGES)}
     dom = max(STAGES, key=lambda s: per_launch[s])
     peaks = load_peaks()
     alg = ALG_BYTES[dom] * B                      # one launch processes B pairs
@@ -590,6 +640,8 @@ def run_ours(args) -> None:
                           "l2": f"working set > L2 ({B} pairs x "
                                 f"{m.workspace_bytes([(W, H, 0)]) / 1e6:.0f} MB)"},
                "g_disp_evals_per_s": disp_evals(total_pairs) / (ms / 1e3) / 1e9,
+               "step_ms": {"min": step_ms[0], "median": step_ms[len(step_ms) // 2],
+                           "max": step_ms[-1]},
                "plain_pairs_per_s": plain, "batch_over_plain": value / plain,
                "stage_ms_per_launch": per_launch, "filled": filled,
                "roofline": roof,
@@ -598,13 +650,15 @@ def run_ours(args) -> None:
                        "h2d_bytes_per_step": B * 2 * WH,
                        "d2h_bytes_per_step": B * 9 * WH},
                "gpu_launches": 4 * K * ((B + 63) // 64)}
-        if ws == 1 and not args.no_extras:
-            out["sparse_c1"] = run_c1(de, local, max(3, K // 2), Wm)
-            out["large_c3"] = run_c3(de, local, max(3, K // 4), Wm)
-            out["batched_c4"] = run_c4(de, local, K, Wm)
-            out["serving_c5"] = run_c5(de, local)
         if ws == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline_sample()
+        if ws == 1 and not args.no_extras:
+            Ke = min(K, 20)
+            out["sparse_c1"] = run_c1(de, local, max(3, Ke // 2), Wm)
+            out["large_c3"] = run_c3(de, local, max(3, Ke // 4), Wm)
+            out["batched_c4"] = run_c4(de, local, Ke, Wm, c4_set)
+            out["serving_c5"] = run_c5(de, local)
+            out["python_entry"] = run_py_entry(local)
         print(json.dumps(out), flush=True)
     if ws > 1:
         import torch.distributed as dist
@@ -614,7 +668,7 @@ def run_ours(args) -> None:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--pairs-per-step", type=int, default=16)

@@ -92,10 +92,10 @@ struct Req {
   int stream = 0, W = 0, H = 0, dmax = 0;
   int band = 0;                        // temporal prior band of its stream at admission
   unsigned planes = 0;                 // DE_PLANE_* the client will read
-  std::vector<uint8_t> L, R;
-  std::vector<float> disp, margin;
-  std::vector<uint8_t> conf, qconf;
-  std::vector<int16_t> q4;
+  // page-locked block holding the inputs and the requested outputs (ReqLayout), kept
+  // with the request when it returns to the pool
+  uint8_t* pin = nullptr;
+  size_t pin_cap = 0;
   double t_submit = 0, t_launch = 0, t_done = 0;
   int status = 1;                      // 1 pending, 0 done, < 0 error code
 };
@@ -103,6 +103,24 @@ struct Req {
 struct Slot {                          // one request's place in a lane's arena
   size_t L, R, disp, margin, conf, q4, qconf;
 };
+
+// A request's page-locked block: L | R | disp | margin | conf | q4 | qconf, each
+// 256-byte aligned, so the inputs move up in one copy into an arena slot laid out the
+// same way and each output plane comes straight back into the block.
+Slot req_layout(int W, int H, size_t* total) {
+  const size_t WH = size_t(W) * H;
+  Slot s;
+  size_t o = 0;
+  s.L = o;       o = align256(o + WH);
+  s.R = o;       o = align256(o + WH);
+  s.disp = o;    o = align256(o + WH * 4);
+  s.margin = o;  o = align256(o + WH * 4);
+  s.conf = o;    o = align256(o + WH);
+  s.q4 = o;      o = align256(o + WH * 2);
+  s.qconf = o;   o = align256(o + WH);
+  if (total) *total = o;
+  return s;
+}
 
 // Arena of one batch: [inputs | outputs | status words] [plain workspace] [one-at-a-
 // time workspace].  Requests of streams without a prior run as one batched launch
@@ -124,9 +142,10 @@ struct Lane {
   cudaStream_t s = nullptr;
   uint8_t* dev = nullptr;              // I/O block, then the pipeline workspaces
   size_t dev_cap = 0;
-  uint8_t* pin = nullptr;              // pinned mirror of the I/O block
+  uint8_t* pin = nullptr;              // page-locked copy of the batch's status words
   size_t pin_cap = 0;
   std::vector<Req*> batch;
+  std::vector<int> status_of;          // per request of a finished batch
   Plan plan;
   bool busy = false;
   bool finished = false;               // set by the stream callback
@@ -172,6 +191,7 @@ struct de_server {
   float* rd_pin = nullptr;
   size_t rd_cap = 0;
   std::vector<Req*> pool;              // finished requests kept with their buffers
+  std::vector<uint8_t*> retired_pin;   // replaced request blocks, freed at destruction
   std::vector<double> lat;
   uint64_t batches = 0, batched_pairs = 0, completed = 0, failed = 0;
   size_t max_pending = 0;
@@ -325,16 +345,14 @@ const float* previous_map(de_server* sv, cudaStream_t s, const Req* r) {
 int launch(de_server* sv, Lane& l) {
   if (!plan_batch(sv, l.batch, &l.plan)) return de::set_error(DE_ERR_ARG, "batch plan");
   const Plan& P = l.plan;
-  std::vector<de::HostCopy> jobs;
-  for (size_t i = 0; i < l.batch.size(); ++i) {
+  cudaError_t e = cudaSuccess;
+  for (size_t i = 0; i < l.batch.size() && e == cudaSuccess; ++i) {
     Req* r = l.batch[i];
-    const size_t WH = size_t(r->W) * r->H;
-    jobs.push_back({l.pin + P.slots[i].L, r->L.data(), WH});
-    jobs.push_back({l.pin + P.slots[i].R, r->R.data(), WH});
+    const Slot rl = req_layout(r->W, r->H, nullptr);
+    e = cudaMemcpyAsync(l.dev + P.slots[i].L, r->pin + rl.L, rl.R + size_t(r->W) * r->H,
+                        cudaMemcpyHostToDevice, l.s);
     r->t_launch = now_ms();
   }
-  de::parallel_copy(jobs);
-  cudaError_t e = cudaMemcpyAsync(l.dev, l.pin, P.in_end, cudaMemcpyHostToDevice, l.s);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(l.dev + P.status, 0, (1 + P.seq.size()) * sizeof(int), l.s);
   if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
@@ -388,46 +406,43 @@ int launch(de_server* sv, Lane& l) {
   for (size_t i = 0; i < l.batch.size() && e == cudaSuccess; ++i) {
     const Req* r = l.batch[i];
     const Slot& s = P.slots[i];
+    const Slot h = req_layout(r->W, r->H, nullptr);
     const size_t WH = size_t(r->W) * r->H;
-    const struct { unsigned bit; size_t off, bytes; } planes[] = {
-        {DE_PLANE_DISP, s.disp, WH * 4}, {DE_PLANE_MARGIN, s.margin, WH * 4},
-        {DE_PLANE_CONF, s.conf, WH}, {DE_PLANE_Q4, s.q4, WH * 2}, {DE_PLANE_QCONF, s.qconf, WH}};
+    const struct { unsigned bit; size_t dev, host, bytes; } planes[] = {
+        {DE_PLANE_DISP, s.disp, h.disp, WH * 4}, {DE_PLANE_MARGIN, s.margin, h.margin, WH * 4},
+        {DE_PLANE_CONF, s.conf, h.conf, WH}, {DE_PLANE_Q4, s.q4, h.q4, WH * 2},
+        {DE_PLANE_QCONF, s.qconf, h.qconf, WH}};
     for (const auto& pl : planes)
       if ((r->planes & pl.bit) && e == cudaSuccess)
-        e = cudaMemcpyAsync(l.pin + pl.off, l.dev + pl.off, pl.bytes, cudaMemcpyDeviceToHost, l.s);
+        e = cudaMemcpyAsync(r->pin + pl.host, l.dev + pl.dev, pl.bytes, cudaMemcpyDeviceToHost,
+                            l.s);
   }
   // the status words (a bounded device wait that ran out sets one)
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(l.pin + P.status, status, (1 + P.seq.size()) * sizeof(int),
+    e = cudaMemcpyAsync(l.pin, status, (1 + P.seq.size()) * sizeof(int),
                         cudaMemcpyDeviceToHost, l.s);
   if (e == cudaSuccess) e = cudaLaunchHostFunc(l.s, lane_done, &l);
   if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "download: %s", cudaGetErrorString(e));
   return DE_OK;
 }
 
-// Copies a finished lane's results into its requests.  Lock held.
-void deliver(de_server* sv, Lane& l) {
+// A finished lane's status words, one per request (the outputs are already in each
+// request's page-locked block).  The server lock is not needed.
+void copy_results(Lane& l) {
   const Plan& P = l.plan;
   std::vector<int> words(1 + P.seq.size());
-  std::memcpy(words.data(), l.pin + P.status, words.size() * sizeof(int));
-  std::vector<int> word_of(l.batch.size(), words[0]);
-  for (size_t q = 0; q < P.seq.size(); ++q) word_of[P.seq[q]] = words[1 + q];
+  std::memcpy(words.data(), l.pin, words.size() * sizeof(int));
+  l.status_of.assign(l.batch.size(), words[0] ? DE_ERR_TIMEOUT : 0);
+  for (size_t q = 0; q < P.seq.size(); ++q)
+    l.status_of[P.seq[q]] = words[1 + q] ? DE_ERR_TIMEOUT : 0;
+}
+
+// Publishes a finished lane's requests and frees the lane.  Lock held.
+void deliver(de_server* sv, Lane& l) {
   const double t = now_ms();
   for (size_t i = 0; i < l.batch.size(); ++i) {
     Req* r = l.batch[i];
-    const Slot& s = P.slots[i];
-    const int status = word_of[i] ? DE_ERR_TIMEOUT : 0;
-    const size_t WH = size_t(r->W) * r->H;
-    auto take = [&](unsigned bit, auto& v, size_t off, size_t esz) {
-      if (!(r->planes & bit)) return;
-      v.resize(WH);
-      std::memcpy(v.data(), l.pin + off, WH * esz);
-    };
-    take(DE_PLANE_DISP, r->disp, s.disp, 4);
-    take(DE_PLANE_MARGIN, r->margin, s.margin, 4);
-    take(DE_PLANE_CONF, r->conf, s.conf, 1);
-    take(DE_PLANE_Q4, r->q4, s.q4, 2);
-    take(DE_PLANE_QCONF, r->qconf, s.qconf, 1);
+    const int status = l.status_of[i];
     r->status = status;
     r->t_done = t;
     if (status) {
@@ -459,6 +474,9 @@ void worker_main(de_server* sv) {
     bool any_busy = false;
     for (Lane& l : sv->lanes) {
       if (l.busy && l.finished) {
+        lk.unlock();
+        copy_results(l);
+        lk.lock();
         deliver(sv, l);
         sv->cv_done.notify_all();
       }
@@ -478,7 +496,8 @@ void worker_main(de_server* sv) {
         }
         b.push_back(front);
         Plan plan;
-        if (!plan_batch(sv, b, &plan) || plan.total > l.dev_cap || plan.io_end > l.pin_cap) {
+        if (!plan_batch(sv, b, &plan) || plan.total > l.dev_cap ||
+            (1 + plan.seq.size()) * sizeof(int) > l.pin_cap) {
           b.pop_back();
           if (b.empty()) {                       // alone it does not fit: refuse it
             Req* r = sv->pending.front();
@@ -501,6 +520,10 @@ void worker_main(de_server* sv) {
       sv->batched_pairs += b.size();
       lk.unlock();
       const int rc = launch(sv, l);
+      // a launch that failed part-way may have copies into its requests' blocks in
+      // flight: let them finish before the requests are handed back (no host callback
+      // of this lane is queued, so this cannot wait on the lock)
+      if (rc) cudaStreamSynchronize(l.s);
       lk.lock();
       if (rc) {
         fail_batch(sv, l, rc);
@@ -566,9 +589,7 @@ int de_server_create(const de_cfg* cfg, const de_server_cfg* scfg, de_server** o
     l.owner = sv;
     cudaError_t e = cudaStreamCreateWithFlags(&l.s, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMalloc(&l.dev, per);
-    // the pinned mirror holds the I/O block only: at most ~14 bytes per pixel of a
-    // pair whose workspace (>= 2*W*H*64 bytes) also fits the arena
-    const size_t pin = std::max<size_t>(per / 8, size_t(16) << 20);
+    const size_t pin = align256((1 + size_t(scfg->max_batch)) * sizeof(int));
     if (e == cudaSuccess) e = cudaHostAlloc(reinterpret_cast<void**>(&l.pin), pin,
                                             cudaHostAllocDefault);
     if (e != cudaSuccess) {
@@ -598,15 +619,41 @@ int de_server_submit(de_server* sv, int stream, const uint8_t* L, const uint8_t*
   probe.dmax = dmax;
   size_t dummy = 0;
   if (int rc = de_dense_workspace_bytes(&sv->cfg, &probe, 1, &dummy)) return rc;
+  size_t need = 0;
+  const Slot rl = req_layout(W, H, &need);
   Req* r = nullptr;
   {
+    // a pooled request whose block is large enough, else any pooled one
     std::lock_guard<std::mutex> lk(sv->mu);
-    if (!sv->pool.empty()) {
-      r = sv->pool.back();
-      sv->pool.pop_back();
+    size_t pick = sv->pool.size();
+    for (size_t i = 0; i < sv->pool.size(); ++i)
+      if (sv->pool[i]->pin_cap >= need &&
+          (pick == sv->pool.size() || sv->pool[i]->pin_cap < sv->pool[pick]->pin_cap))
+        pick = i;
+    if (pick == sv->pool.size() && !sv->pool.empty()) pick = sv->pool.size() - 1;
+    if (pick < sv->pool.size()) {
+      r = sv->pool[pick];
+      sv->pool.erase(sv->pool.begin() + long(pick));
     }
   }
   if (!r) r = new Req;
+  if (r->pin_cap < need) {
+    // a bigger block; the old one is freed with the server (freeing page-locked memory
+    // can wait for the device, which this submitting thread should not)
+    uint8_t* nb = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&nb), need, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->pool.push_back(r);
+      return de::set_error(DE_ERR_OOM, "page-locked request buffer of %zu bytes", need);
+    }
+    if (r->pin) {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->retired_pin.push_back(r->pin);
+    }
+    r->pin = nb;
+    r->pin_cap = need;
+  }
   r->planes = planes ? planes : DE_PLANE_ALL;
   r->status = 1;
   r->stream = stream;
@@ -614,15 +661,13 @@ int de_server_submit(de_server* sv, int stream, const uint8_t* L, const uint8_t*
   r->H = H;
   r->dmax = dmax;
   const size_t WH = size_t(W) * H;
-  r->L.resize(WH);
-  r->R.resize(WH);
-  std::memcpy(r->L.data(), L, WH);
-  std::memcpy(r->R.data(), R, WH);
+  std::memcpy(r->pin + rl.L, L, WH);
+  std::memcpy(r->pin + rl.R, R, WH);
   r->t_submit = now_ms();
   {
     std::lock_guard<std::mutex> lk(sv->mu);
     if (sv->stop) {
-      delete r;
+      sv->pool.push_back(r);
       return de::set_error(DE_ERR_CLOSED, "server is shutting down");
     }
     r->ticket = sv->next_ticket++;
@@ -650,17 +695,22 @@ int de_server_wait(de_server* sv, unsigned long long ticket, int timeout_ms, flo
                            (unsigned long long)ticket, timeout_ms);
   const int status = r->status;
   if (status == 0) {
+    // the copies run in the caller's thread without the lock: the request stays
+    // registered (so nothing reuses it) until they are done
+    lk.unlock();
     const size_t WH = size_t(r->W) * r->H;
     const unsigned p = r->planes;
-    if (disp && (p & DE_PLANE_DISP)) std::memcpy(disp, r->disp.data(), WH * 4);
-    if (margin && (p & DE_PLANE_MARGIN)) std::memcpy(margin, r->margin.data(), WH * 4);
-    if (conf && (p & DE_PLANE_CONF)) std::memcpy(conf, r->conf.data(), WH);
-    if (q4 && (p & DE_PLANE_Q4)) std::memcpy(q4, r->q4.data(), WH * 2);
-    if (qconf && (p & DE_PLANE_QCONF)) std::memcpy(qconf, r->qconf.data(), WH);
+    const Slot h = req_layout(r->W, r->H, nullptr);
+    if (disp && (p & DE_PLANE_DISP)) std::memcpy(disp, r->pin + h.disp, WH * 4);
+    if (margin && (p & DE_PLANE_MARGIN)) std::memcpy(margin, r->pin + h.margin, WH * 4);
+    if (conf && (p & DE_PLANE_CONF)) std::memcpy(conf, r->pin + h.conf, WH);
+    if (q4 && (p & DE_PLANE_Q4)) std::memcpy(q4, r->pin + h.q4, WH * 2);
+    if (qconf && (p & DE_PLANE_QCONF)) std::memcpy(qconf, r->pin + h.qconf, WH);
     if (latency_ms) *latency_ms = r->t_done - r->t_submit;
+    lk.lock();
   }
   sv->reqs.erase(it);
-  if (sv->pool.size() < 256) sv->pool.push_back(r); else delete r;
+  sv->pool.push_back(r);
   if (status) return de::set_error(status, "request failed (%d)", status);
   return DE_OK;
 }
@@ -765,8 +815,15 @@ int de_server_destroy(de_server* sv) {
   for (float* p : sv->retired) cudaFree(p);
   if (sv->rd_pin) cudaFreeHost(sv->rd_pin);
   if (sv->state_s) cudaStreamDestroy(sv->state_s);
-  for (auto& kv : sv->reqs) delete kv.second;
-  for (Req* r : sv->pool) delete r;
+  for (auto& kv : sv->reqs) {
+    if (kv.second->pin) cudaFreeHost(kv.second->pin);
+    delete kv.second;
+  }
+  for (Req* r : sv->pool) {
+    if (r->pin) cudaFreeHost(r->pin);
+    delete r;
+  }
+  for (uint8_t* p : sv->retired_pin) cudaFreeHost(p);
   delete sv;
   return DE_OK;
 }

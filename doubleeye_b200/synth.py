@@ -246,13 +246,25 @@ BATCH_SHAPES = {(320, 240): 64, (640, 480): 128, (848, 480): 128, (1280, 720): 2
                 (1920, 1080): 256}
 
 
-def batch_pairs(n=64, seed=BASE_SEED, shapes=None):
-    """n pairs with sizes drawn uniformly (seed-fixed) from BATCH_SHAPES, each from
-    the slanted-plane generator with disparity range 0..D-1 matched to its size."""
+def _slanted_job(args):
+    W, H, dmax, seed, tag = args
+    return slanted_planes(W, H, dmax, seed=seed, tag=tag)
+
+
+def batch_pairs(n=64, seed=BASE_SEED, shapes=None, workers: int = 0):
+    """n distinct pairs with sizes drawn uniformly (seed-fixed) from BATCH_SHAPES, each
+    from the slanted-plane generator (its own seed) with disparity range 0..D-1
+    matched to its size.  workers > 1 generates them in that many spawned processes
+    (the same pairs, in the same order)."""
     shapes = list((shapes or BATCH_SHAPES).items())
     rng = rng_for("batch-draw", seed)
-    out = []
+    jobs = []
     for i in range(n):
         (W, H), D = shapes[int(rng.integers(0, len(shapes)))]
-        out.append(slanted_planes(W, H, D - 1, seed=seed + i, tag=f"batch{i}"))
-    return out
+        jobs.append((W, H, D - 1, seed + i, f"batch{i}"))
+    if workers > 1:
+        import concurrent.futures as cf
+        import multiprocessing as mp
+        with cf.ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_slanted_job, jobs))
+    return [_slanted_job(j) for j in jobs]

@@ -571,6 +571,7 @@ def run_ours(args) -> None:
         m.match_into(one)
     torch.cuda.synchronize()
     barrier(ws)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(K):
         m.match_into(one)

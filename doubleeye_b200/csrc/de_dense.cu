@@ -55,16 +55,10 @@ __device__ __forceinline__ int find_pair(const int* prefix, int n, int item) {
   return lo;
 }
 
-// One recursive-filter step (core/tools/de_dense.cpp:419):
-//   c + ((a (f - c) + 2^14) >> 15)  with an int32 carry and an arithmetic shift.
-// Computed as (c (2^15 - a) + a f + 2^14) >> 15, the same integer: c 2^15 is a
-// multiple of 2^15, so adding it before or after the shift is exact, and the sum is a
-// convex combination of c and f scaled by 2^15, so for int16 c and f and a in
-// [0, 2^15) it stays within +-2^30 (no int32 overflow).  The term in c does not
-// depend on the carried f, so the chain from one step to the next is one
-// multiply-add and one shift.
+// One recursive-filter step (core/tools/de_dense.cpp:419): int32 carry, +2^14
+// rounding, arithmetic shift.
 __device__ __forceinline__ int32_t rf_step(int32_t c, int32_t f, int32_t a) {
-  return (a * f + (c * ((1 << 15) - a) + (1 << 14))) >> 15;
+  return c + ((a * (f - c) + (1 << 14)) >> 15);
 }
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
@@ -697,9 +691,8 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
       pk1 = 0;                                        // key 0 never displaces a candidate
 #pragma unroll
       for (int s = 0; s < KT; ++s) {
-        // (v + 32768) << 8 | (255 - k) as one multiply-add: v + 32768 is in [0, 2^16)
         const uint32_t key =
-            (s < nvalid) ? uint32_t(st[s]) * 256u + uint32_t((32768 << 8) + 255 - k0 - s) : 0u;
+            (s < nvalid) ? (uint32_t(st[s] + 32768) << 8) | uint32_t(255 - k0 - s) : 0u;
         const uint32_t lo = min(pk0, key);
         pk0 = max(pk0, key);
         pk1 = max(pk1, lo);

@@ -836,16 +836,16 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   const float lambda = cfg.lambda, gamma = cfg.gamma, damping = cfg.damping, keep = cfg.keep;
   // Candidate state lives in bucket-sorted POSITION order: the members of a right
   // pixel's bucket are contiguous, candidates that claim no right pixel follow them.
-  // Shared bytes per pixel: cs 8, beta 8, rho 8, claim 8, start 4, item 4, pos 4,
+  // Shared bytes per pixel: cs 8, beta 8, rho 8, lohi 8, start 4, item 4, pos 4,
   // cd 2, rev 2, cn 1 = 49 (five rows per SM at W = 848).  Arrays that are never
   // live together share storage: the sort cursors live in beta until beta is
   // cleared, pixel-order cs in rho until the sort, and the claim stage's best,
-  // bestj and win in the claim block after the BP sweeps.
+  // bestj and win in lohi, which only the BP sweeps read.
   float* __restrict__ s_cs = reinterpret_cast<float*>(smem);          // [2W] by position
   float* __restrict__ s_beta = s_cs + 2 * W;                           // [2W] by position
   float* __restrict__ s_rho = s_beta + 2 * W;                          // [2W] by position (pixel-order cs first)
-  int* __restrict__ s_claim = reinterpret_cast<int*>(s_rho + 2 * W);   // [2W] claim stage
-  int* s_start = s_claim + 2 * W;                         // [W+1]
+  int* __restrict__ s_lohi = reinterpret_cast<int*>(s_rho + 2 * W);    // [2W] bucket bounds lo | hi << 16, -1 none
+  int* s_start = s_lohi + 2 * W;                          // [W+1]
   int16_t* s_item = reinterpret_cast<int16_t*>(s_start + W + 1);   // [2W] position -> 2x + j
   int16_t* s_pos = s_item + 2 * W;                        // [2W] 2x + j -> position
   uint8_t* s_cd = reinterpret_cast<uint8_t*>(s_pos + 2 * W);  // [2W] k (valid for j < cn)
@@ -853,8 +853,8 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   int8_t* s_cn = reinterpret_cast<int8_t*>(s_rev + W);    // [W]
   float* s_cspx = s_rho;                                  // pixel-order cs until the sort
   int* s_cur = reinterpret_cast<int*>(s_beta);            // [W] sort cursors until beta is cleared
-  float* s_best = reinterpret_cast<float*>(s_claim);      // [W] after the BP sweeps
-  int8_t* s_bestj = reinterpret_cast<int8_t*>(s_claim + W);    // [W] after the BP sweeps
+  float* s_best = reinterpret_cast<float*>(s_lohi);       // [W] after the BP sweeps
+  int8_t* s_bestj = reinterpret_cast<int8_t*>(s_lohi + W);     // [W] after the BP sweeps
   uint8_t* s_win = reinterpret_cast<uint8_t*>(s_bestj + W);    // [W] after the BP sweeps
   __shared__ int warp_sums[kSolveThreads / 32];
   __shared__ int s_nitems, s_extra;
@@ -919,15 +919,17 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
     const int n = s_cn[x];
     for (int j = 0; j < n; ++j) {
       const int xr = x - (dmin + s_cd[2 * x + j]);
-      int p;
+      int p, lohi = -1;
       if (xr >= 0) {
         p = atomicAdd(&s_cur[xr], 1);
+        lohi = s_start[xr] | (s_start[xr + 1] << 16);
       } else {
         p = nitems + atomicAdd(&s_extra, 1);
       }
       s_item[p] = int16_t(2 * x + j);
       s_pos[2 * x + j] = int16_t(p);
       s_cs[p] = s_cspx[2 * x + j];
+      s_lohi[p] = lohi;
     }
   }
   __syncthreads();
@@ -976,24 +978,23 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
       }
     }
     __syncthreads();
-    // beta per right pixel's bucket: one pass for its best and runner-up rho (the
-    // reference's Top2, first maximum kept), then each member's "largest rho of the
-    // others" is the runner-up for the best and the best for everyone else -- the same
-    // float as the maximum over the others, in one pass instead of one per member
-    for (int xr = tid; xr < W; xr += kSolveThreads) {
-      const int lo = s_start[xr], hi = s_start[xr + 1];
-      if (hi <= lo) continue;
-      float b1 = kNegBig, b2 = kNegBig;
-      int i1 = -1;
-      for (int r = lo; r < hi; ++r) {
-        const float v = s_rho[r];
-        if (v > b1) { b2 = b1; b1 = v; i1 = r; }
-        else if (v > b2) b2 = v;
+    for (int p = tid; p < nitems; p += kSolveThreads) {
+      const int lohi = s_lohi[p];
+      const int lo = lohi & 0xFFFF, hi = lohi >> 16;     // p's bucket, hi > lo
+      // The first four members are read at once and reduced as a tree; fmax_ref
+      // keeps its left operand on ties, so the tree returns the scan's first
+      // maximum, and members past the fourth continue the scan from it.
+      float v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int r = lo + u;
+        const float t = s_rho[min(r, hi - 1)];
+        v[u] = (r < hi && r != p) ? t : kNegBig;
       }
-      for (int r = lo; r < hi; ++r) {
-        const float ex = (r == i1) ? b2 : b1;
-        s_beta[r] = keep * (s_cs[r] - fmax_ref(gamma, ex)) + damping * s_beta[r];
-      }
+      float ex = fmax_ref(fmax_ref(v[0], v[1]), fmax_ref(v[2], v[3]));
+      for (int r = lo + 4; r < hi; ++r)
+        if (r != p) ex = fmax_ref(ex, s_rho[r]);
+      s_beta[p] = keep * (s_cs[p] - fmax_ref(gamma, ex)) + damping * s_beta[p];
     }
   }
   __syncthreads();

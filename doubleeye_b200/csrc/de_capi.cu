@@ -99,6 +99,7 @@ void make_dev_cfg(const de_cfg& c, DevCfg* o) {
   o->keep = 1.f - c.damping;
   o->min_margin = c.min_margin;
   o->min_ratio = c.min_ratio;
+  o->expire_polls = de::get_expire_polls();
   const int nbits = census_bits(c);
   o->packed = nbits <= 48;
   const int half = nbits / 2;
@@ -545,6 +546,7 @@ int de_set_param(const char* name, int value) {
   if (!std::strcmp(name, "cols_pf")) { de::set_cols_pf(value); return DE_OK; }
   if (!std::strcmp(name, "cols_cta")) { de::set_cols_cta(value); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { de::set_solve_threads(value); return DE_OK; }
+  if (!std::strcmp(name, "expire_wait_polls")) { de::set_expire_polls(value); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 
@@ -555,6 +557,7 @@ int de_get_param(const char* name, int* value) {
   if (!std::strcmp(name, "cols_pf")) { *value = de::get_cols_pf(); return DE_OK; }
   if (!std::strcmp(name, "cols_cta")) { *value = de::get_cols_cta(); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { *value = de::get_solve_threads(); return DE_OK; }
+  if (!std::strcmp(name, "expire_wait_polls")) { *value = de::get_expire_polls(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 

@@ -298,8 +298,9 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
   return done != 0;
 }
 constexpr int kWaitLimit = 1 << 22;                  // try_wait rounds before giving up
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err) {
-  for (int i = 0; i < kWaitLimit; ++i)
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity, int* err,
+                                          int limit = kWaitLimit) {
+  for (int i = 0; i < limit; ++i)
     if (mbar_test(bar, parity)) return;
   if (err) atomicExch(err, 1);
 }
@@ -517,6 +518,12 @@ __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
       slot = (slot + 1 == NS) ? 0 : slot + 1;
     }
   }
+  // Test hook (knob "expire_wait_polls"): once every real wait has completed and no
+  // copy is in flight, the launch's first CTA waits a bounded number of polls on the
+  // spare barrier, which nothing arrives at, so the time-out path of a device wait and
+  // the status it reports are exercised without a fault.
+  if (cfg.expire_polls > 0 && blockIdx.x == 0 && tid == 0)
+    mbar_wait(&bars[3], 0u, err, cfg.expire_polls);
 }
 
 // ---------------------------------------------------------------------------------
@@ -1309,6 +1316,10 @@ cudaError_t launch_cols_t(const DevCfg& cfg, const Batch& b, const de_cfg_hw& hw
   if (nt == 128) return launch_cols_nt<KT, TPCP, 128>(cfg, b, hwc, s);
   return launch_cols_nt<KT, TPCP, 256>(cfg, b, hwc, s);
 }
+
+int g_expire_polls = 0;
+void set_expire_polls(int v) { g_expire_polls = v < 0 ? 0 : (v > (1 << 20) ? (1 << 20) : v); }
+int get_expire_polls() { return g_expire_polls; }
 
 void set_cols_pf(int v) { g_cols_pf = (v == 4 || v == 8 || v == 16) ? v : 0; }
 int get_cols_pf() { return g_cols_pf; }

@@ -57,6 +57,7 @@ struct DevCfg {
   int packed;          // census words carry the pixel byte (window <= 48 bits)
   int subpixel, fit_eq, lrc;
   float lambda, gamma, damping, keep, min_margin, min_ratio;
+  int expire_polls;    // test hook (knob "expire_wait_polls"), 0 = off
   int16_t tbl[66];     // Q14 census score per Hamming distance
   int16_t adt[256];    // Q14 truncated-absolute-difference score
   uint16_t rf[256];    // Q15 filter coefficient per byte difference
@@ -107,6 +108,8 @@ void set_cols_pf(int v);
 int get_cols_pf();
 void set_cols_cta(int v);
 int get_cols_cta();
+void set_expire_polls(int v);
+int get_expire_polls();
 cudaError_t launch_export_candidates(const DevCfg& cfg, const Batch& b, cudaStream_t s);
 // The prior-masked cost stage (de_prior.cu): one pair (b.p[0]) after its census.
 size_t prior_ws_bytes(int W, int H, int D);

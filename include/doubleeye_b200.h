@@ -177,7 +177,14 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *                       pairs or less, else 256)
  *   "solve_threads"     threads per image row in the row solve: 128, 256, 512, or
  *                       0 to choose by row width (default 0: 512 for rows wider
- *                       than 1024 pixels, else 256) */
+ *                       than 1024 pixels, else 256)
+ * and one test hook that does change results:
+ *   "expire_wait_polls" 0 (default) or a poll count: every row-kernel launch then
+ *                       ends, after all its real waits have completed, with a
+ *                       bounded wait of that many polls on a barrier nothing
+ *                       arrives at, so the launch set reports a device wait that ran
+ *                       out (DE_ERR_TIMEOUT / a non-zero workspace status) without any
+ *                       fault; for testing callers' handling of that status */
 DE_API int de_set_param(const char* name, int value);
 DE_API int de_get_param(const char* name, int* value);
 

@@ -261,50 +261,6 @@ void timer_mark(cudaStream_t s, std::vector<cudaEvent_t>* group) {
   }
 }
 
-// Streams the disparity groups of a batch run on, beside the caller's: one set per
-// thread, device and calling stream (so batches issued on different streams, such as
-// the host context's chunks, do not queue behind one another), created on first use.
-struct GroupStreams {
-  cudaStream_t s[4] = {};
-  cudaEvent_t fork = nullptr, done[4] = {};
-  bool ok = false;
-};
-
-GroupStreams* group_streams(cudaStream_t origin) {
-  thread_local std::unordered_map<int, std::unordered_map<cudaStream_t, GroupStreams>> sets;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  GroupStreams& g = sets[dev][origin];
-  if (!g.ok) {
-    cudaError_t e = cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming);
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
-      e = cudaStreamCreateWithFlags(&g.s[i], cudaStreamNonBlocking);
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done[i], cudaEventDisableTiming);
-    }
-    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
-    g.ok = true;
-  }
-  return &g;
-}
-
-// The pairs of b whose Dpad is 64 G, with their work-item prefixes.
-void group_batch(const de::Batch& b, int G, de::Batch* out) {
-  de::Batch& g = *out;
-  g = b;
-  g.n = 0;
-  g.maxDpad = 64 * G;
-  g.rows_prefix[0] = g.cols_prefix[0] = g.solve_prefix[0] = g.pix_prefix[0] = 0;
-  for (int i = 0; i < b.n; ++i) {
-    if (b.p[i].Dpad != 64 * G) continue;
-    const int k = g.n++;
-    g.p[k] = b.p[i];
-    g.rows_prefix[k + 1] = g.rows_prefix[k] + (b.rows_prefix[i + 1] - b.rows_prefix[i]);
-    g.cols_prefix[k + 1] = g.cols_prefix[k] + (b.cols_prefix[i + 1] - b.cols_prefix[i]);
-    g.solve_prefix[k + 1] = g.solve_prefix[k] + (b.solve_prefix[i + 1] - b.solve_prefix[i]);
-    g.pix_prefix[k + 1] = g.pix_prefix[k] + (b.pix_prefix[i + 1] - b.pix_prefix[i]);
-  }
-}
-
 int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
   de::DevCfg dc;
   de::make_dev_cfg(c, &dc);
@@ -317,35 +273,6 @@ int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
   const bool timed = g_timer.on && cap == cudaStreamCaptureStatusNone;
   if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_census(dc, b, s));
-  // A batch that mixes disparity groups (Dpad 64, 128, 192, 256) runs each group's
-  // rows -> columns -> solve chain on its own stream after the census, so one group's
-  // tail overlaps the next group's work instead of idling the SMs between launches.
-  // Pairs are independent, so the results are those of the sequential order.
-  bool present[5] = {};
-  int groups = 0;
-  for (int i = 0; i < b.n; ++i) {
-    const int G = b.p[i].Dpad / 64;
-    if (!present[G]) { present[G] = true; ++groups; }
-  }
-  GroupStreams* gs = (!timed && groups > 1) ? group_streams(s) : nullptr;
-  if (gs) {
-    thread_local de::Batch sub;
-    DE_CUDA(cudaEventRecord(gs->fork, s));
-    int k = 0;
-    for (int G = 4; G >= 1; --G) {                     // the widest group first
-      if (!present[G]) continue;
-      group_batch(b, G, &sub);
-      cudaStream_t t = gs->s[k];
-      DE_CUDA(cudaStreamWaitEvent(t, gs->fork, 0));
-      DE_CUDA(de::launch_rows(dc, sub, t));
-      DE_CUDA(de::launch_cols(dc, sub, t));
-      DE_CUDA(de::launch_solve(dc, sub, false, t));
-      DE_CUDA(cudaEventRecord(gs->done[k], t));
-      DE_CUDA(cudaStreamWaitEvent(s, gs->done[k], 0));
-      ++k;
-    }
-    return DE_OK;
-  }
   if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_rows(dc, b, s));
   if (timed) timer_mark(s, &grp);

@@ -509,6 +509,15 @@ def run_c3(de, local: int, steps: int, warmup: int) -> dict:
     return out
 
 
+def launch_sets(n: int) -> int:
+    """Census/rows/columns/solve launch sets one batch of n pairs runs as: batches of at
+    most 64 pairs, each split into up to `batch_streams` parts on concurrent streams."""
+    from doubleeye_b200 import _lib
+    parts = _lib.get_param("batch_streams")
+    return sum(min(m, parts) for m in
+               (min(64, n - first) for first in range(0, n, 64)))
+
+
 def run_ours(args) -> None:
     import torch
     import doubleeye_b200 as de
@@ -650,7 +659,7 @@ def run_ours(args) -> None:
                "e2e": {"value": ws * B * K / e2e_s, "unit": "pairs/s",
                        "h2d_bytes_per_step": B * 2 * WH,
                        "d2h_bytes_per_step": B * 9 * WH},
-               "gpu_launches": 4 * K * ((B + 63) // 64)}
+               "gpu_launches": 4 * K * launch_sets(B)}
         if ws == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline_sample()
         if ws == 1 and not args.no_extras:

@@ -9,6 +9,7 @@ onto the GPU, so every setting gives bit-identical results:
   cols_cta          column-kernel threads per CTA (0 = by batch size)
   solve_threads     threads per row in the row solve, the BP schedule's width (0 = by
                     row width)
+  batch_streams     parts a batch runs as on concurrent streams
 
 ``tune`` times a batch under a coordinate-descent search over these values (CUDA
 events, warm-up first) and returns the fastest setting; ``Tuner`` caches the choice
@@ -29,6 +30,7 @@ KNOBS = {
     "cols_pf": [0, 4, 8, 16],
     "cols_cta": [0, 128, 256],
     "solve_threads": [0, 128, 256, 512],
+    "batch_streams": [1, 2, 3, 4],
 }
 CACHE = os.path.join(_lib.PKG, "_lib", "autotune.json")
 

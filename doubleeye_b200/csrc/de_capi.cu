@@ -261,7 +261,56 @@ void timer_mark(cudaStream_t s, std::vector<cudaEvent_t>* group) {
   }
 }
 
-int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
+// Streams a batch's parts run on, beside the caller's: one set per thread, device and
+// calling stream (so batches issued on different streams, such as the host context's
+// chunks, do not queue behind one another), created on first use with the calling
+// stream's priority.
+struct PartStreams {
+  cudaStream_t s[4] = {};
+  cudaEvent_t fork = nullptr, done[4] = {};
+  bool ok = false;
+};
+
+PartStreams* part_streams(cudaStream_t origin) {
+  thread_local std::unordered_map<int, std::unordered_map<cudaStream_t, PartStreams>> sets;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  PartStreams& g = sets[dev][origin];
+  if (!g.ok) {
+    int prio = 0;
+    cudaError_t e = cudaStreamGetPriority(origin, &prio);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+      e = cudaStreamCreateWithPriority(&g.s[i], cudaStreamNonBlocking, prio);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    g.ok = true;
+  }
+  return &g;
+}
+
+// Pairs k, k + parts, k + 2 parts, ... of b, with their work-item prefixes.
+void part_batch(const de::Batch& b, int parts, int k, de::Batch* out) {
+  de::Batch& g = *out;
+  g = b;
+  g.n = 0;
+  g.maxDpad = 0;
+  g.rows_prefix[0] = g.cols_prefix[0] = g.solve_prefix[0] = g.pix_prefix[0] = 0;
+  for (int i = k; i < b.n; i += parts) {
+    const int j = g.n++;
+    g.p[j] = b.p[i];
+    g.maxDpad = std::max(g.maxDpad, b.p[i].Dpad);
+    g.rows_prefix[j + 1] = g.rows_prefix[j] + (b.rows_prefix[i + 1] - b.rows_prefix[i]);
+    g.cols_prefix[j + 1] = g.cols_prefix[j] + (b.cols_prefix[i + 1] - b.cols_prefix[i]);
+    g.solve_prefix[j + 1] = g.solve_prefix[j] + (b.solve_prefix[i + 1] - b.solve_prefix[i]);
+    g.pix_prefix[j + 1] = g.pix_prefix[j] + (b.pix_prefix[i + 1] - b.pix_prefix[i]);
+  }
+}
+
+int g_batch_streams = 2;          // parts a batch of several pairs is run as, 1..4
+
+int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s, int max_parts) {
   de::DevCfg dc;
   de::make_dev_cfg(c, &dc);
   if (c.lrc)
@@ -271,6 +320,29 @@ int run_batch(const de_cfg& c, de::Batch& b, cudaStream_t s) {
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(s, &cap);
   const bool timed = g_timer.on && cap == cudaStreamCaptureStatusNone;
+  // A batch of several pairs runs as up to max_parts parts (pairs taken in turn), each
+  // part's census -> rows -> columns -> solve chain on its own stream, so one part's
+  // kernel tails overlap another part's work instead of idling SMs between launches.
+  // Pairs are independent, so the results are the single chain's.  With stage timing
+  // on, the stages run in order on the caller's stream.
+  const int parts = std::min(b.n, max_parts);
+  PartStreams* ps = (!timed && parts > 1) ? part_streams(s) : nullptr;
+  if (ps) {
+    thread_local de::Batch sub;
+    DE_CUDA(cudaEventRecord(ps->fork, s));
+    for (int k = 0; k < parts; ++k) {
+      part_batch(b, parts, k, &sub);
+      cudaStream_t t = ps->s[k];
+      DE_CUDA(cudaStreamWaitEvent(t, ps->fork, 0));
+      DE_CUDA(de::launch_census(dc, sub, t));
+      DE_CUDA(de::launch_rows(dc, sub, t));
+      DE_CUDA(de::launch_cols(dc, sub, t));
+      DE_CUDA(de::launch_solve(dc, sub, false, t));
+      DE_CUDA(cudaEventRecord(ps->done[k], t));
+      DE_CUDA(cudaStreamWaitEvent(s, ps->done[k], 0));
+    }
+    return DE_OK;
+  }
   if (timed) timer_mark(s, &grp);
   DE_CUDA(de::launch_census(dc, b, s));
   if (timed) timer_mark(s, &grp);
@@ -362,12 +434,20 @@ int de_dense_workspace_bytes(const de_cfg* cfg, const de_pair* pairs, int n,
 
 int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace,
                  size_t ws_bytes, void* stream) {
+  return de::dense_dev(cfg, pairs, n, workspace, ws_bytes, static_cast<cudaStream_t>(stream),
+                       g_batch_streams);
+}
+
+}  // extern "C"
+
+int de::dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace,
+                  size_t ws_bytes, cudaStream_t stream, int max_parts) {
   size_t need = 0;
   int rc = de_dense_workspace_bytes(cfg, pairs, n, &need);
   if (rc) return rc;
   if (need > ws_bytes || (need && !workspace))
     return fail(DE_ERR_ARG, "workspace %zu bytes, need %zu", ws_bytes, need);
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaStream_t s = stream;
   uint8_t* ws = static_cast<uint8_t*>(workspace);
   int* err = reinterpret_cast<int*>(ws);
   ws += de::kStatusBytes;
@@ -381,10 +461,12 @@ int de_dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace
     for (int i = 0; i < m; ++i)
       ws += de::pair_workspace_bytes(pairs[first + i].W, pairs[first + i].H,
                                      pair_D(*cfg, pairs[first + i]), cfg->lrc != 0);
-    if ((rc = run_batch(*cfg, b, s))) return rc;
+    if ((rc = run_batch(*cfg, b, s, max_parts))) return rc;
   }
   return DE_OK;
 }
+
+extern "C" {
 
 int de_dense_prior_workspace_bytes(const de_cfg* cfg, const de_pair* pair, size_t* bytes) {
   if (!bytes || !pair) return fail(DE_ERR_ARG, "NULL argument");
@@ -547,6 +629,10 @@ int de_set_param(const char* name, int value) {
   if (!std::strcmp(name, "cols_cta")) { de::set_cols_cta(value); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { de::set_solve_threads(value); return DE_OK; }
   if (!std::strcmp(name, "expire_wait_polls")) { de::set_expire_polls(value); return DE_OK; }
+  if (!std::strcmp(name, "batch_streams")) {
+    g_batch_streams = std::min(4, std::max(1, value));
+    return DE_OK;
+  }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 
@@ -558,6 +644,7 @@ int de_get_param(const char* name, int* value) {
   if (!std::strcmp(name, "cols_cta")) { *value = de::get_cols_cta(); return DE_OK; }
   if (!std::strcmp(name, "solve_threads")) { *value = de::get_solve_threads(); return DE_OK; }
   if (!std::strcmp(name, "expire_wait_polls")) { *value = de::get_expire_polls(); return DE_OK; }
+  if (!std::strcmp(name, "batch_streams")) { *value = g_batch_streams; return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 
@@ -847,8 +934,10 @@ int de_ctx_dense_batch(de_ctx* c, const de_pair* hp, int n) {
     for (int k = 0; k < nch; ++k) {
       cudaStream_t sk = c->cs[k];
       if (k > 0) DE_CUDA(cudaStreamWaitEvent(sk, c->ev_in[k], 0));
-      if ((r = de_dense_dev(&c->cfg, dp.data() + bound[k], bound[k + 1] - bound[k],
-                            dws + woff[k], woff[k + 1] - woff[k], sk)))
+      // chunks already overlap one another: each runs as one launch set
+      if ((r = de::dense_dev(&c->cfg, dp.data() + bound[k], bound[k + 1] - bound[k],
+                             dws + woff[k], woff[k + 1] - woff[k], sk,
+                             nch > 1 ? 1 : g_batch_streams)))
         return r;
       DE_CUDA(cudaMemcpyAsync(&hstat[k], dws + woff[k], sizeof(int), cudaMemcpyDeviceToHost, sk));
       DE_CUDA(cudaEventRecord(c->ev_done[k], sk));

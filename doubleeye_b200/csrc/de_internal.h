@@ -74,6 +74,12 @@ struct Batch {
   DevPair p[kMaxBatch];
 };
 
+// de_dense_dev with a bound on the parts a batch runs as on concurrent streams (1: one
+// launch set on `stream`); callers that already overlap batches of their own pass 1
+// (de_capi.cu).
+int dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace,
+              size_t ws_bytes, cudaStream_t stream, int max_parts);
+
 // Device address of the no-allocation entry point's status word on the current device
 // (de_noalloc.cu); DE_OK or an error code already recorded for de_last_error().
 int noalloc_status_word(void** out);

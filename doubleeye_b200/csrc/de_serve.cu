@@ -370,8 +370,9 @@ int launch(de_server* sv, Lane& l) {
   if (!P.plain.empty()) {
     std::vector<de_pair> dp;
     for (int i : P.plain) dp.push_back(device_pair(l, l.batch[i], P.slots[i]));
-    if (int rc = de_dense_dev(&sv->cfg, dp.data(), int(dp.size()), l.dev + P.ws_plain,
-                              P.ws_plain_bytes, l.s))
+    // the lanes already overlap one another's batches: one launch set each
+    if (int rc = de::dense_dev(&sv->cfg, dp.data(), int(dp.size()), l.dev + P.ws_plain,
+                               P.ws_plain_bytes, l.s, 1))
       return rc;
     e = cudaMemcpyAsync(status, l.dev + P.ws_plain, sizeof(int), cudaMemcpyDeviceToDevice, l.s);
     if (e != cudaSuccess) return de::set_error(DE_ERR_CUDA, "status: %s", cudaGetErrorString(e));

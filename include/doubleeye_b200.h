@@ -178,6 +178,13 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *   "solve_threads"     threads per image row in the row solve: 128, 256, 512, or
  *                       0 to choose by row width (default 0: 512 for rows wider
  *                       than 1024 pixels, else 256)
+ *   "batch_streams"     1..4 (default 2): de_dense_dev runs a batch of several
+ *                       pairs as that many parts, pairs taken in turn, each part's
+ *                       launch set on its own stream forked from and joined back to
+ *                       the caller's (also under graph capture), so one part's kernel
+ *                       tails overlap the other's work.  The host context's chunked
+ *                       batches and the server's lanes, which already overlap, run
+ *                       each batch as one launch set; stage timing does too
  * and one test hook that does change results:
  *   "expire_wait_polls" 0 (default) or a poll count: every row-kernel launch then
  *                       ends, after all its real waits have completed, with a

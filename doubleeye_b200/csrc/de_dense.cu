@@ -722,19 +722,17 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
       pk0 = max(pk0, o0);
       pk1 = max(max(pk1, o1), lo);
     };
-    // every lane of the group holds the merged keys; lane 0 writes them
+    // a lane holding a row's merged keys writes them, with the winner's neighbours
     auto emit = [&](int y, uint32_t pk0, uint32_t pk1, const int16_t* rowbuf) {
       const int kw = pk0 ? 255 - int(pk0 & 255u) : -1;
       const int32_t vm = rowbuf[max(kw - 1, 0)];
       const int32_t vp = rowbuf[min(kw + 1, kRowbufLast)];
       const int32_t nm = (kw >= 1) ? vm : -32768;
       const int32_t np = (kw >= 0 && kw + 1 <= kmax) ? vp : -32768;
-      if (sub == 0 && colok) {
-        const size_t i = size_t(y) * W + x;
-        P.key0[i] = pk0;
-        P.key1[i] = pk1;
-        P.nb[i] = pk16(nm, np);
-      }
+      const size_t i = size_t(y) * W + x;
+      P.key0[i] = pk0;
+      P.key1[i] = pk1;
+      P.nb[i] = pk16(nm, np);
     };
     auto bwd = [&](int y, int j) {                   // one row
       uint32_t pk0, pk1;
@@ -743,22 +741,44 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
 #pragma unroll
       for (int off = TPCP / 2; off > 0; off >>= 1) merge_step(pk0, pk1, off);
       __syncwarp(gmask);
-      emit(y, pk0, pk1, rowbufs[0]);
+      if (sub == 0 && colok) emit(y, pk0, pk1, rowbufs[0]);
     };
-    // kRB rows at a time: their lane merges are independent (only the filter state
-    // runs from row to row), so the shuffle chains interleave.
+    // kRB rows at a time, merged across the group's lanes by recursive halving: in
+    // round t lanes h = TPCP >> (t + 1) apart pair up, each keeps half of the rows it
+    // holds (the upper half where its bit h is set) and merges its partner's partial
+    // keys for them, so after log2(kRB) rounds lane `sub` holds row sub / (TPCP /
+    // kRB) alone, merged over kRB lanes; a butterfly over the remaining TPCP / kRB
+    // lanes finishes it.  That is 2 kRB - 1 merges a lane (kRB log2(TPCP) with a
+    // butterfly per row), and kRB lanes write the kRB rows side by side.  The merge
+    // is order-free, so the result is the sequential scan's.
+    static_assert(TPCP >= kRB, "each lane ends with one row");
+    constexpr int kLanesPerRow = TPCP / kRB;
     auto bwdn = [&](int y, int j) {                   // rows y, y - 1, ..., y - kRB + 1
       uint32_t k0s[kRB], k1s[kRB];
       __syncwarp(gmask);
 #pragma unroll
       for (int r = 0; r < kRB; ++r) row_keys(y - r, j + r, k0s[r], k1s[r], rowbufs[r]);
 #pragma unroll
-      for (int off = TPCP / 2; off > 0; off >>= 1)
+      for (int h = TPCP / 2, half = kRB / 2; half > 0; h >>= 1, half >>= 1) {
+        const bool up = (sub & h) != 0;
 #pragma unroll
-        for (int r = 0; r < kRB; ++r) merge_step(k0s[r], k1s[r], off);
+        for (int i = 0; i < half; ++i) {
+          const uint32_t s0 = up ? k0s[i] : k0s[i + half];
+          const uint32_t s1 = up ? k1s[i] : k1s[i + half];
+          const uint32_t m0 = up ? k0s[i + half] : k0s[i];
+          const uint32_t m1 = up ? k1s[i + half] : k1s[i];
+          const uint32_t o0 = __shfl_xor_sync(gmask, s0, h, TPCP);
+          const uint32_t o1 = __shfl_xor_sync(gmask, s1, h, TPCP);
+          const uint32_t lo = min(m0, o0);
+          k0s[i] = max(m0, o0);
+          k1s[i] = max(max(m1, o1), lo);
+        }
+      }
+#pragma unroll
+      for (int off = kLanesPerRow / 2; off > 0; off >>= 1) merge_step(k0s[0], k1s[0], off);
       __syncwarp(gmask);
-#pragma unroll
-      for (int r = 0; r < kRB; ++r) emit(y - r, k0s[r], k1s[r], rowbufs[r]);
+      const int r = sub / kLanesPerRow;
+      if (sub % kLanesPerRow == 0 && colok) emit(y - r, k0s[0], k1s[0], &sbuf[wib][r][gbase * KT]);
     };
 #pragma unroll
     for (int j = 0; j < PF; ++j) {

@@ -272,12 +272,32 @@ def cpu_baseline_sample(reps: int = 5) -> dict:
     spread = lambda v: {"min_s": min(v), "median_s": sorted(v)[len(v) // 2],  # noqa: E731
                         "max_s": max(v)}
     return {"value": 1.0 / min(t_all), "unit": "pairs/s", "cores": nthreads, "kind": kind,
-            "cpu_model": cpu_model(),
+            "cpu_model": cpu_model(), "python_entry": py_entry_cpu(),
             "single_thread_pairs_per_s": 1.0 / min(t_one),
             "all_threads": spread(t_all), "one_thread": spread(t_one),
             "sample": f"one 848x480 D=128 iters 8 pair, {reps} interleaved repetitions at "
                       f"{nthreads} and 1 thread(s), minimum reported, "
                       f"{'reference run_dense' if kind == 'reference' else 'oracle port'}"}
+
+
+def py_entry_cpu(iters: int = 3) -> dict:
+    """The Python entry points' max-sum (article/masda_stereo.py masda_sparse, float64)
+    on one host core: the oracle's C restatement over the same 450x375, disparities
+    1..60 edge list the GPU leg solves (built by this build's dense_problem, which is
+    bit-exact to the reference's), for `iters` of the 12 iterations, and the 12-iteration
+    time scaled from them."""
+    import numpy as np
+    from doubleeye_b200 import dense_masda, synth
+    from oracle import oracle as O
+    p = synth.slanted_planes(450, 375, 59, seed=11, tag="py-entry")
+    ei, ej, se, n = dense_masda.dense_problem(p.left, p.right, 1, 60)
+    se = se.astype(np.float64)
+    orc = O.Oracle()
+    t0 = time.perf_counter()
+    orc.masda_edges(ei, ej, se, n, n, -0.1, -0.1, iters, 0.4, 1e-9)
+    t = time.perf_counter() - t0
+    return {"kind": "port", "cores": 1, "edges": int(se.shape[0]), "iterations_timed": iters,
+            "masda_sparse_ms": t * 1e3, "masda_sparse_12_iterations_ms_scaled": t * 1e3 * 12 / iters}
 
 
 def run_reference(args) -> None:

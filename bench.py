@@ -657,6 +657,13 @@ def run_ours(args) -> None:
             if st in ALG_POPC:
                 r["popc_frac"] = ALG_POPC[st] * B / t / 1e12 / popc_peak
             roof["int_roof"][st] = r
+    # the row solve has neither an HBM nor an integer roof worth the name (12 bytes in
+    # and 9 out per pixel): it is bound by latency, one CTA per image row holding the
+    # row's candidates in shared memory (49 bytes per pixel, five rows per SM at 848
+    # pixels), with two block barriers per BP sweep
+    roof["solve"] = {"us_per_pair": per_launch["solve"] * 1e3 / B, "bp_sweeps": ITERS,
+                     "bound": "latency: shared-memory round trips and 2 block barriers "
+                              "per BP sweep, 5 rows per SM"}
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": ws, "steps": K,

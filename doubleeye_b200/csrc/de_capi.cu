@@ -261,33 +261,66 @@ void timer_mark(cudaStream_t s, std::vector<cudaEvent_t>* group) {
   }
 }
 
-// Streams a batch's parts run on, beside the caller's: one set per thread, device and
-// calling stream (so batches issued on different streams, such as the host context's
-// chunks, do not queue behind one another), created on first use with the calling
-// stream's priority.
+// Streams a batch's parts run on, beside the caller's.  Each thread keeps, per
+// device, a few sets of them, each set serving one calling stream at a time (so
+// batches issued on different streams, such as a caller's own pipelined streams, do
+// not queue behind one another).  A calling stream without a set takes over the set
+// used least recently (never one whose streams are part of an open graph capture):
+// its streams are reused as they are, so at worst the new caller's parts order
+// behind work still queued from the old one.  The table never grows, however many
+// streams a caller cycles through; with no set free the batch runs as one launch set.
 struct PartStreams {
+  cudaStream_t origin = nullptr;
+  unsigned long long used = 0;
   cudaStream_t s[4] = {};
   cudaEvent_t fork = nullptr, done[4] = {};
   bool ok = false;
 };
 
 PartStreams* part_streams(cudaStream_t origin) {
-  thread_local std::unordered_map<int, std::unordered_map<cudaStream_t, PartStreams>> sets;
+  constexpr int kSets = 4;
+  struct Table { PartStreams set[kSets]; unsigned long long clock = 0; };
+  thread_local std::unordered_map<int, Table> tables;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
-  PartStreams& g = sets[dev][origin];
-  if (!g.ok) {
+  Table& t = tables[dev];
+  PartStreams* g = nullptr;
+  for (PartStreams& c : t.set)
+    if (c.ok && c.origin == origin) g = &c;
+  if (!g) {
+    // a set whose streams still belong to an open graph capture is not taken over
+    auto capturing = [](const PartStreams& c) {
+      for (cudaStream_t x : c.s) {
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (x && (cudaStreamIsCapturing(x, &st) != cudaSuccess ||
+                  st != cudaStreamCaptureStatusNone)) {
+          cudaGetLastError();
+          return true;
+        }
+      }
+      return false;
+    };
+    for (PartStreams& c : t.set) {
+      if (!c.ok) { g = &c; break; }
+      if ((!g || c.used < g->used) && !capturing(c)) g = &c;
+    }
+    if (!g) return nullptr;                           // every set busy in a capture
+  }
+  if (!g->ok) {
     int prio = 0;
     cudaError_t e = cudaStreamGetPriority(origin, &prio);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess && !g->fork) e = cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming);
     for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
-      e = cudaStreamCreateWithPriority(&g.s[i], cudaStreamNonBlocking, prio);
-      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done[i], cudaEventDisableTiming);
+      if (!g->s[i]) e = cudaStreamCreateWithPriority(&g->s[i], cudaStreamNonBlocking, prio);
+      if (e == cudaSuccess && !g->done[i])
+        e = cudaEventCreateWithFlags(&g->done[i], cudaEventDisableTiming);
     }
-    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }
-    g.ok = true;
+    if (e != cudaSuccess) { cudaGetLastError(); return nullptr; }   // kept for a retry
+    g->ok = true;
   }
-  return &g;
+  g->origin = origin;
+  g->used = ++t.clock;
+  return g;
 }
 
 // Pairs k, k + parts, k + 2 parts, ... of b, with their work-item prefixes.

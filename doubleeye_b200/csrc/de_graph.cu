@@ -1,11 +1,13 @@
 // A batch's launch set captured once as a CUDA graph and replayed.
 //
 // The dense pipeline for a fixed batch layout (pair sizes, disparity ranges, input,
-// output and workspace buffers) is five stream operations: a status-word reset and
-// four kernels whose descriptors travel as kernel parameters.  Capturing them turns a
-// repeated batch (a camera rig's frames, a fixed-size benchmark batch) into one graph
-// launch, so the host pays one launch per batch instead of one per kernel.  Replays
-// read whatever the captured input buffers hold at replay time.
+// output and workspace buffers) is a status-word reset and the four kernels of each
+// launch set, whose descriptors travel as kernel parameters (a batch of several pairs
+// runs as two launch sets on streams forked from the capturing stream and joined back
+// to it, which the graph keeps as two branches).  Capturing them turns a repeated
+// batch (a camera rig's frames, a fixed-size benchmark batch) into one graph launch,
+// so the host pays one launch per batch instead of one per kernel.  Replays read
+// whatever the captured input buffers hold at replay time.
 
 #include <cuda_runtime.h>
 

@@ -178,3 +178,38 @@ def test_host_batch_chunks_equal_single_pairs(de):
         for key in ("disp", "margin", "conf"):
             a, b = getattr(got[k], key), getattr(one, key)
             assert same(torch.from_numpy(np.ascontiguousarray(a)), torch.from_numpy(b)), (k, key)
+
+
+def test_batches_on_many_streams_and_a_capture(de, batch):
+    """A batch of several pairs runs as parts on streams forked from the caller's; each
+    thread keeps a few such sets and hands the least recently used one to a new calling
+    stream.  Nine calling streams in turn, then a graph captured on a tenth while the
+    others keep launching, all give the one-stream results."""
+    pairs, Ls, Rs = batch
+    ref = run(de, de.DenseMatcher(de.Cfg(iters=4)), Ls, Rs, cand=False)
+    items_for = lambda m: [(L, R, D, m.new_outputs(*L.shape))  # noqa: E731
+                           for L, R, (_, _, D) in zip(Ls, Rs, SHAPES)]
+    streams = [torch.cuda.Stream() for _ in range(9)]
+    mats = [de.DenseMatcher(de.Cfg(iters=4)) for _ in streams]
+    items = [items_for(m) for m in mats]
+    for rnd in range(2):
+        for st, m, it in zip(streams, mats, items):
+            st.wait_stream(torch.cuda.current_stream())
+            m.match_into(it, stream=st)
+    torch.cuda.synchronize()
+    for it in items:
+        for k in range(len(SHAPES)):
+            for key in ("disp", "margin", "conf"):
+                assert same(it[k][3][key], ref[k][key]), (k, key)
+    mc = de.DenseMatcher(de.Cfg(iters=4))
+    cit = items_for(mc)
+    g = mc.capture(cit)
+    for st, m, it in zip(streams, mats, items):       # other streams launch meanwhile
+        m.match_into(it, stream=st)
+    g.launch()
+    torch.cuda.synchronize()
+    for k in range(len(SHAPES)):
+        for key in ("disp", "margin", "conf"):
+            assert same(cit[k][3][key], ref[k][key]), (k, key)
+            assert same(items[0][k][3][key], ref[k][key]), (k, key)
+    g.close()

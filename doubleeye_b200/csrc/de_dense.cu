@@ -315,12 +315,20 @@ __device__ __forceinline__ void fence_proxy_async() {
 // the x-coefficients, read by both passes, are double-buffered.  Forward results go
 // to the volume with plain stores; the backward pass brings them back through a
 // ring of bulk copies, so no thread waits on a global load.
+// Backward ring: stages of kRowsChunk disparity-columns (x times Dpad, 4 KB), two in
+// flight.  Two 4 KB stages rather than three keep a row's shared footprint at 27 KB
+// at D = 128, so eight rows fit an SM instead of seven (rows 0.935 -> 0.861 ms per 16
+// pairs); smaller stages lose more to the per-stage barrier than the extra row
+// gains (2 KB stages, nine rows: 0.971 ms).
+constexpr int kRowsChunk = 2048;
+constexpr int kRowsRing = 2;
+
 template <bool PACKED, int TS, int G>
 __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
   constexpr int DP = 64 * G;                          // Dpad
   constexpr int XS = DP / 2;                          // x stride in 32-bit words
-  constexpr int CH = 2048 / DP;                       // x columns per backward chunk
-  constexpr int NS = 3;                               // backward ring depth
+  constexpr int CH = kRowsChunk / DP;                 // x columns per backward chunk
+  constexpr int NS = kRowsRing;                       // backward ring depth
   constexpr size_t STAGE = size_t(CH) * DP * 2;
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t bars[4 + NS];      // census, ax[2], spare, ring
@@ -1196,7 +1204,7 @@ size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   size_t s = size_t(TS) * 64 * 2;
   s += size_t(cpm) * 16;
   s += 2 * ((size_t(apm) * 2 + 127) & ~size_t(127));
-  s += size_t(3) * (2048 / (64 * G)) * (64 * G) * 2;
+  s += size_t(kRowsRing) * (kRowsChunk / (64 * G)) * (64 * G) * 2;
   if (!packed) s += size_t(maxW) * 2;
   return (s + 15) & ~size_t(15);
 }

@@ -315,20 +315,21 @@ __device__ __forceinline__ void fence_proxy_async() {
 // the x-coefficients, read by both passes, are double-buffered.  Forward results go
 // to the volume with plain stores; the backward pass brings them back through a
 // ring of bulk copies, so no thread waits on a global load.
-// Backward ring: stages of kRowsChunk disparity-columns (x times Dpad, 4 KB), two in
-// flight.  Two 4 KB stages rather than three keep a row's shared footprint at 27 KB
-// at D = 128, so eight rows fit an SM instead of seven (rows 0.935 -> 0.861 ms per 16
-// pairs); smaller stages lose more to the per-stage barrier than the extra row
-// gains (2 KB stages, nine rows: 0.971 ms).
+// Backward ring: stages of kRowsChunk disparity-columns (x times Dpad, 4 KB), two or
+// three in flight (NS).  The launcher takes two where that puts more rows
+// in flight at Dpad <= 128 (at 848x480 D=128 the footprint falls from 31 to 27 KB and
+// eight rows fit an SM instead of seven: rows 0.935 -> 0.861 ms per 16 pairs as one
+// launch set), else three, which hide the copies better.  Smaller
+// stages lose more to the per-stage barrier than an extra row gains (2 KB stages,
+// nine rows: 0.971 ms).
 constexpr int kRowsChunk = 2048;
-constexpr int kRowsRing = 2;
 
-template <bool PACKED, int TS, int G>
+template <bool PACKED, int TS, int G, int NS>
 __global__ void __launch_bounds__(32 * G, 8 / G) k_rows(DevCfg cfg, Batch b) {
   constexpr int DP = 64 * G;                          // Dpad
   constexpr int XS = DP / 2;                          // x stride in 32-bit words
   constexpr int CH = kRowsChunk / DP;                 // x columns per backward chunk
-  constexpr int NS = kRowsRing;                       // backward ring depth
+
   constexpr size_t STAGE = size_t(CH) * DP * 2;
   extern __shared__ __align__(128) uint8_t smem[];
   __shared__ __align__(8) uint64_t bars[4 + NS];      // census, ax[2], spare, ring
@@ -1194,7 +1195,7 @@ __global__ void k_export(DevCfg cfg, Batch b) {
   }
 }
 
-size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
+size_t rows_smem(const Batch& b, int TS, int G, bool packed, int ring) {
   int cpm = 0, apm = 0, maxW = 0;
   for (int i = 0; i < b.n; ++i) {
     cpm = std::max(cpm, b.p[i].cpitch);
@@ -1204,7 +1205,7 @@ size_t rows_smem(const Batch& b, int TS, int G, bool packed) {
   size_t s = size_t(TS) * 64 * 2;
   s += size_t(cpm) * 16;
   s += 2 * ((size_t(apm) * 2 + 127) & ~size_t(127));
-  s += size_t(kRowsRing) * (kRowsChunk / (64 * G)) * (64 * G) * 2;
+  s += size_t(ring) * (kRowsChunk / (64 * G)) * (64 * G) * 2;
   if (!packed) s += size_t(maxW) * 2;
   return (s + 15) & ~size_t(15);
 }
@@ -1243,18 +1244,44 @@ int g_cols_pf = 0;                // rows the column kernel prefetches: 4, 8, 16
 
 template <bool PACKED, int TS, int G>
 cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
-  const size_t sm = rows_smem(b, TS, G, PACKED);
-  cudaError_t e = set_smem(k_rows<PACKED, TS, G>, sm);
-  if (e != cudaSuccess) return e;
+  auto kern2 = k_rows<PACKED, TS, G, 2>;
+  auto kern3 = k_rows<PACKED, TS, G, 3>;
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  int fit = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, k_rows<PACKED, TS, G>, 32 * G, sm);
-  const int per_sm = std::max(1, std::min(fit > 0 ? fit : 1, g_rows_ctas_per_sm));
+  // rows in flight with two and with three backward stages.  Two only where they put
+  // more rows in flight (a batch with fewer rows than the SMs hold either way keeps
+  // three), and only up to Dpad 128: measured per shape, the extra row per SM gains
+  // 2.5% at 320x240 D=64 and the 848x480 D=128 bench batch, and loses 1-2% at 1280x720
+  // and 1920x1080 D=256, where a row's stage is 4 columns wide.  The occupancy of each
+  // footprint is looked up once per kernel and size.
+  struct Occ { const void* k; size_t sm; int fit; };
+  thread_local std::vector<Occ> occ_cache;
+  auto fit_of = [&](auto kern, size_t sm) -> int {
+    for (const Occ& o : occ_cache)
+      if (o.k == reinterpret_cast<const void*>(kern) && o.sm == sm) return o.fit;
+    int fit = 0;
+    if (set_smem(kern, sm) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&fit, kern, 32 * G, sm) != cudaSuccess) {
+      cudaGetLastError();
+      fit = 1;
+    }
+    if (occ_cache.size() > 64) occ_cache.clear();
+    occ_cache.push_back({reinterpret_cast<const void*>(kern), sm, fit});
+    return fit;
+  };
+  const size_t sm2 = rows_smem(b, TS, G, PACKED, 2), sm3 = rows_smem(b, TS, G, PACKED, 3);
+  const int per2 = std::max(1, std::min(fit_of(kern2, sm2), g_rows_ctas_per_sm));
+  const int per3 = std::max(1, std::min(fit_of(kern3, sm3), g_rows_ctas_per_sm));
   const int items = b.rows_prefix[b.n];
-  const int grid = std::min(items, per_sm * nsm);
-  k_rows<PACKED, TS, G><<<grid, 32 * G, sm, s>>>(cfg, b);
+  cudaError_t e;
+  if (G <= 2 && std::min(items, per2 * nsm) > std::min(items, per3 * nsm)) {
+    if ((e = set_smem(kern2, sm2)) != cudaSuccess) return e;
+    kern2<<<std::min(items, per2 * nsm), 32 * G, sm2, s>>>(cfg, b);
+  } else {
+    if ((e = set_smem(kern3, sm3)) != cudaSuccess) return e;
+    kern3<<<std::min(items, per3 * nsm), 32 * G, sm3, s>>>(cfg, b);
+  }
   return cudaGetLastError();
 }
 

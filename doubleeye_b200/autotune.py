@@ -10,6 +10,7 @@ onto the GPU, so every setting gives bit-identical results:
   solve_threads     threads per row in the row solve, the BP schedule's width (0 = by
                     row width)
   batch_streams     parts a batch runs as on concurrent streams
+  cols_async        column-kernel prefetch through shared memory (1) or registers (0)
 
 ``tune`` times a batch under a coordinate-descent search over these values (CUDA
 events, warm-up first) and returns the fastest setting; ``Tuner`` caches the choice
@@ -31,6 +32,7 @@ KNOBS = {
     "cols_cta": [0, 128, 256],
     "solve_threads": [0, 128, 256, 512],
     "batch_streams": [1, 2, 3, 4],
+    "cols_async": [1, 0],
 }
 CACHE = os.path.join(_lib.PKG, "_lib", "autotune.json")
 

@@ -666,6 +666,7 @@ int de_set_param(const char* name, int value) {
     g_batch_streams = std::min(4, std::max(1, value));
     return DE_OK;
   }
+  if (!std::strcmp(name, "cols_async")) { de::set_cols_async(value); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 
@@ -678,6 +679,7 @@ int de_get_param(const char* name, int* value) {
   if (!std::strcmp(name, "solve_threads")) { *value = de::get_solve_threads(); return DE_OK; }
   if (!std::strcmp(name, "expire_wait_polls")) { *value = de::get_expire_polls(); return DE_OK; }
   if (!std::strcmp(name, "batch_streams")) { *value = g_batch_streams; return DE_OK; }
+  if (!std::strcmp(name, "cols_async")) { *value = de::get_cols_async(); return DE_OK; }
   return fail(DE_ERR_ARG, "unknown parameter %s", name);
 }
 

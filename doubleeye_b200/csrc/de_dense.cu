@@ -20,9 +20,10 @@
 //             copies.
 //   k_cols    a column is a group of lanes, each lane KT disparities: vertical
 //             forward pass written in place, vertical backward pass fused with the
-//             top-2 (packed keys, a butterfly over the group) and the winner's
-//             neighbour costs; rows stream through per-lane register rings, with
-//             no block-wide step.
+//             top-2 (packed keys, merged over the group by recursive halving) and
+//             the winner's neighbour costs; rows stream through per-lane rings (in
+//             shared memory filled by cp.async at 8 disparities per lane, else in
+//             registers), with no block-wide step.
 //   k_solve   one CTA per row: candidate buckets by right pixel, damped max-sum
 //             iterations, belief, and the one-to-one claim done in parallel as a
 //             per-right-pixel arg-max (each pixel claims exactly one right pixel,
@@ -557,10 +558,15 @@ __device__ __forceinline__ uint32_t pk16(int32_t lo, int32_t hi) {
 // four, and any merge order gives the sequential scan's answer.  The winner's
 // neighbour costs are read back from a per-group row buffer.
 //
-// No block-wide step: each lane reads its own 2*KT bytes of a row straight from
-// global memory, PF rows ahead of use through a register ring (the rows of a warp's
-// columns are adjacent, so a warp's loads and stores of one row are contiguous), and
-// the only synchronisation is the group's own merge of a column's lanes.  Warps
+// No block-wide step: each lane reads its own 2*KT bytes of a row from global memory,
+// PF rows ahead of use (the rows of a warp's columns are adjacent, so a warp's loads
+// and stores of one row are contiguous), and the only synchronisation is the group's
+// own merge of a column's lanes.  At 8 disparities per lane (AS) the ring is the
+// lane's own 16-byte slots in shared memory, filled by cp.async and read after
+// cp.async.wait_group: it needs no registers, so the kernel runs at 80 registers and
+// three 256-thread CTAs per SM (two with a register ring), and a concurrent launch
+// set finds room beside it (the 16-pair batch 2.53 -> 2.41 ms, 1280x720 D=256 4.76 ->
+// 4.43 ms); the kernel alone times the same.  Otherwise the ring is in registers.  Warps
 // therefore run at their own pace instead of meeting at a barrier every row.  A lane
 // reads back only what it stored itself in the forward pass.  Only the filter state
 // runs from row to row, so the backward pass merges several rows' keys together
@@ -591,9 +597,26 @@ __device__ __forceinline__ void vstore(uint32_t* p, const uint32_t* w) {
   }
 }
 
-template <int KT, int TPCP, int PF, int NT>
-__global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
+// Ampere-style asynchronous copies (cp.async) of 16 bytes into shared memory, counted
+// in commit groups; each lane copies and later reads only its own slots.  The source
+// operand `dep` only orders the copy after the register it names is ready (the slot's
+// previous contents have been read into it).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t dep) {
+  asm volatile("{ .reg .b32 d; mov.b32 d, %2; cp.async.cg.shared.global [%0], [%1], 16; }"
+               ::"r"(smem_addr(dst)), "l"(src), "r"(dep) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int KT, int TPCP, int PF, int NT, bool AS = false>
+__global__ void __launch_bounds__(NT, (AS ? 768 : 512) / NT) k_cols(DevCfg cfg, Batch b) {
   static_assert((KT == 4 || KT % 8 == 0) && TPCP >= 1 && TPCP <= 32, "shape");
+  static_assert(!AS || KT == 8, "the asynchronous ring moves 16 bytes a lane and row");
   constexpr int KW = KT / 2;                         // 32-bit words per lane and row
   constexpr int NCOL = NT / TPCP;                    // columns per CTA tile
   // backward rows whose lane merges run together: 8 where the prefetch ring is 8 or
@@ -602,6 +625,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   // lane (more would spill)
   constexpr int kRB = KT >= 16 ? 2 : (PF >= 8 ? 8 : 4);
   __shared__ __align__(16) int16_t sbuf[NT / 32][kRB][32 * KT];   // kRB row buffers per warp
+  // AS: the prefetch ring in (dynamic) shared memory, PF slots of 16 bytes per lane,
+  // so it costs no registers (more warps per SM) and no barrier (a lane reads only its
+  // own slots); per warp, slot j of lane l is word (j * 32 + l) * KW
+  extern __shared__ __align__(16) uint32_t sring[];
   const int tid = threadIdx.x, lane = tid & 31, wib = tid >> 5;
   const int gi = tid / TPCP, sub = tid % TPCP, gbase = lane - sub;
   const unsigned gmask = (TPCP == 32) ? 0xffffffffu : (((1u << TPCP) - 1u) << gbase);
@@ -645,17 +672,41 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   auto fetch = [&](int y, uint32_t* dst) { vload<KW>(gcol + size_t(y) * grs, dst); };
   // The steady-state loops below run whole blocks of PF rows with no branch, so a
   // load issued PF rows ahead stays in flight until its row; a guarded tail finishes.
-  uint32_t ring[PF][KW] = {};
+  uint32_t ring[AS ? 1 : PF][KW] = {};
   int32_t aring[PF] = {};
+  // ring slot j: take the row it holds (AS: once its copy group has landed; one group
+  // per row, rows taken in issue order, so PF - 1 newer groups may stay in flight) and
+  // refill it with row y
+  uint32_t* const myslot = AS ? sring + wib * (PF * 32 * KW) + lane * KW : nullptr;
+  auto ring_take = [&](int j, uint32_t* c) {
+    if constexpr (AS) {
+      cp_async_wait<PF - 1>();
+      const uint4 v = *reinterpret_cast<const uint4*>(myslot + j * 32 * KW);
+      c[0] = v.x; c[1] = v.y; c[2] = v.z; c[3] = v.w;
+    } else {
+#pragma unroll
+      for (int i = 0; i < KW; ++i) c[i] = ring[j][i];
+    }
+  };
+  auto ring_fill = [&](int j, int y, uint32_t dep) {
+    if constexpr (AS) {
+      cp_async16(myslot + j * 32 * KW, gcol + size_t(y) * grs, dep);
+      cp_async_commit();
+    } else {
+      fetch(y, ring[j]);
+    }
+  };
   const int ylast = clampi(yin - 1, 0, H - 1);        // last row with input
   // ---- vertical forward, rows hh..H-1, results stored in place --------------------
   auto fwd = [&](int y, int j) {
     uint32_t c[KW];
+    ring_take(j, c);
+    const uint32_t dep = c[0];
 #pragma unroll
-    for (int i = 0; i < KW; ++i) c[i] = (y < yin) ? ring[j][i] : 0u;
+    for (int i = 0; i < KW; ++i) c[i] = (y < yin) ? c[i] : 0u;
     const int32_t a = aring[j];
     const int yn = y + PF;
-    fetch(min(yn, ylast), ring[j]);
+    ring_fill(j, min(yn, ylast), dep);
     aring[j] = ay[size_t(min(yn, H - 1)) * W];
     step(c, a);
     if (live) {
@@ -666,7 +717,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   };
 #pragma unroll
   for (int j = 0; j < PF; ++j) {
-    fetch(min(hh + j, ylast), ring[j]);
+    ring_fill(j, min(hh + j, ylast), 0u);
     aring[j] = ay[size_t(min(hh + j, H - 1)) * W];
   }
   int y0 = hh;
@@ -677,6 +728,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
 #pragma unroll
   for (int j = 0; j < PF; ++j)
     if (y0 + j < H) fwd(y0 + j, j);
+  if constexpr (AS) cp_async_wait<0>();               // the forward's last refills land
   // ---- vertical backward from H-1 (its value is the forward one) + top-2 ----------
   // Rows yin..H-2 carry no candidates: plain steps with direct loads.
   int ys = H - 2;
@@ -696,11 +748,10 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
     // buffer (for the winner's neighbours).
     auto row_keys = [&](int y, int j, uint32_t& pk0, uint32_t& pk1, int16_t* rowbuf) {
       uint32_t c[KW];
-#pragma unroll
-      for (int i = 0; i < KW; ++i) c[i] = ring[j][i];
+      ring_take(j, c);
       const int32_t a = aring[j];
       const int yn = y - PF;
-      fetch(max(yn, 0), ring[j]);
+      ring_fill(j, max(yn, 0), c[0]);
       aring[j] = ay[size_t(max(yn + 1, 0)) * W];
       step(c, a);
       pk0 = 0;
@@ -791,7 +842,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
     };
 #pragma unroll
     for (int j = 0; j < PF; ++j) {
-      fetch(max(ys - j, 0), ring[j]);
+      ring_fill(j, max(ys - j, 0), 0u);
       aring[j] = ay[size_t(max(ys - j + 1, 0)) * W];   // coefficient at y + 1
     }
     int yb = ys;
@@ -806,6 +857,7 @@ __global__ void __launch_bounds__(NT, 512 / NT) k_cols(DevCfg cfg, Batch b) {
   };
   if (P.rkey) bwd_rows(std::integral_constant<bool, true>());
   else bwd_rows(std::integral_constant<bool, false>());
+  if constexpr (AS) cp_async_wait<0>();               // no copy outlives the CTA
 }
 
 // ---------------------------------------------------------------------------------
@@ -1241,6 +1293,7 @@ struct de_cfg_hw { int hw, dmin; };
 int g_rows_ctas_per_sm = 32;      // upper bound on row CTAs per SM (rows in flight)
 int g_solve_threads = 0;          // threads per row in the solve: 128, 256, 512, 0 = by width
 int g_cols_pf = 0;                // rows the column kernel prefetches: 4, 8, 16, 0 = by shape
+int g_cols_async = 1;             // 8-row prefetch through shared memory (cp.async)
 
 template <bool PACKED, int TS, int G>
 cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
@@ -1348,6 +1401,15 @@ cudaError_t launch_cols_nt(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& 
       return cudaGetLastError();
     }
   }
+  if constexpr (KT == 8) {
+    if (pf >= 8 && g_cols_async) {                    // the ring in shared memory
+      constexpr size_t ring_bytes = size_t(NT) * 8 * (KT / 2) * 4;
+      const cudaError_t e = set_smem(k_cols<KT, TPCP, 8, NT, true>, ring_bytes);
+      if (e != cudaSuccess) return e;
+      k_cols<KT, TPCP, 8, NT, true><<<tiles, NT, ring_bytes, s>>>(cfg, b);
+      return cudaGetLastError();
+    }
+  }
   if constexpr (KT == 4 || (KT == 8 && TPCP <= 16)) {
     if (pf >= 8) {
       k_cols<KT, TPCP, 8, NT><<<tiles, NT, 0, s>>>(cfg, b);
@@ -1377,6 +1439,8 @@ void set_expire_polls(int v) { g_expire_polls = v < 0 ? 0 : (v > (1 << 20) ? (1 
 int get_expire_polls() { return g_expire_polls; }
 
 void set_cols_pf(int v) { g_cols_pf = (v == 4 || v == 8 || v == 16) ? v : 0; }
+void set_cols_async(int v) { g_cols_async = v ? 1 : 0; }
+int get_cols_async() { return g_cols_async; }
 int get_cols_pf() { return g_cols_pf; }
 
 int g_cols_kt = 0;                // 0 = by batch size, else 4, 8 or 16 disparities per lane

@@ -110,6 +110,8 @@ void set_cols_kt(int v);
 void set_solve_threads(int v);
 int get_solve_threads();
 int get_cols_kt();
+void set_cols_async(int v);
+int get_cols_async();
 void set_cols_pf(int v);
 int get_cols_pf();
 void set_cols_cta(int v);

@@ -178,6 +178,10 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *   "solve_threads"     threads per image row in the row solve: 128, 256, 512, or
  *                       0 to choose by row width (default 0: 512 for rows wider
  *                       than 1024 pixels, else 256)
+ *   "cols_async"        1 (default) or 0: at 8 disparities per lane the column
+ *                       kernel's 8-row prefetch goes through shared memory by
+ *                       asynchronous copies (fewer registers, so more warps and more
+ *                       room for a concurrent launch set) instead of a register ring
  *   "batch_streams"     1..4 (default 2): de_dense_dev runs a batch of several
  *                       pairs as that many parts, pairs taken in turn, each part's
  *                       launch set on its own stream forked from and joined back to

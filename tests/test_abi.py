@@ -102,7 +102,7 @@ def test_workspace_sizing_and_argument_checks(lib):
 
 def test_params_roundtrip(lib):
     for name in ("rows_ctas_per_sm", "cols_kt", "cols_pf", "cols_cta", "solve_threads",
-                 "batch_streams"):
+                 "batch_streams", "cols_async"):
         v = lib.get_param(name)
         lib.set_param(name, v)
         assert lib.get_param(name) == v

@@ -39,7 +39,7 @@ def test_real_win_is_kept(autotune, monkeypatch):
     undo = restore(autotune)
     try:
         autotune.apply({"rows_ctas_per_sm": 32, "cols_kt": 0, "cols_pf": 0, "cols_cta": 0,
-                        "solve_threads": 0, "batch_streams": 2})
+                        "solve_threads": 0, "batch_streams": 2, "cols_async": 1})
         cost = lambda k: 10.0 - (1.0 if k["cols_kt"] == 16 else 0.0) \
             - (0.5 if k["solve_threads"] == 512 else 0.0)
         monkeypatch.setattr(autotune, "_time", fake_timer(autotune, cost))
@@ -55,7 +55,7 @@ def test_one_off_fast_reading_is_rejected(autotune, monkeypatch):
     undo = restore(autotune)
     try:
         start = {"rows_ctas_per_sm": 32, "cols_kt": 0, "cols_pf": 0, "cols_cta": 0,
-                 "solve_threads": 0, "batch_streams": 2}
+                 "solve_threads": 0, "batch_streams": 2, "cols_async": 1}
         autotune.apply(start)
         lucky = dict(start, cols_cta=128)
         noise = {tuple(sorted(lucky.items())): 9.0}        # 10% faster once, by chance

@@ -85,7 +85,7 @@ def test_graph_replay_matches_direct_launch(de, batch):
 
 
 @pytest.mark.parametrize("knob", ["rows_ctas_per_sm", "cols_kt", "cols_pf", "cols_cta",
-                                  "solve_threads", "batch_streams"])
+                                  "solve_threads", "batch_streams", "cols_async"])
 def test_knobs_never_change_results(de, batch, knob):
     from doubleeye_b200 import autotune
     pairs, Ls, Rs = batch

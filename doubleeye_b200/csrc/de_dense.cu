@@ -317,12 +317,10 @@ __device__ __forceinline__ void fence_proxy_async() {
 // to the volume with plain stores; the backward pass brings them back through a
 // ring of bulk copies, so no thread waits on a global load.
 // Backward ring: stages of kRowsChunk disparity-columns (x times Dpad, 4 KB), two or
-// three in flight (NS).  The launcher takes two where that puts more rows
-// in flight at Dpad <= 128 (at 848x480 D=128 the footprint falls from 31 to 27 KB and
-// eight rows fit an SM instead of seven: rows 0.935 -> 0.861 ms per 16 pairs as one
-// launch set), else three, which hide the copies better.  Smaller
-// stages lose more to the per-stage barrier than an extra row gains (2 KB stages,
-// nine rows: 0.971 ms).
+// three in flight (NS).  The launcher takes two where that puts more rows in flight
+// at Dpad 64, else three, which hide the copies better.  Smaller stages lose more to
+// the per-stage barrier than an extra row gains (2 KB stages, nine rows per SM at
+// 848x480 D=128: rows 0.935 -> 0.971 ms per 16 pairs).
 constexpr int kRowsChunk = 2048;
 
 template <bool PACKED, int TS, int G, int NS>
@@ -1304,10 +1302,12 @@ cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   // rows in flight with two and with three backward stages.  Two only where they put
   // more rows in flight (a batch with fewer rows than the SMs hold either way keeps
-  // three), and only up to Dpad 128: measured per shape, the extra row per SM gains
-  // 2.5% at 320x240 D=64 and the 848x480 D=128 bench batch, and loses 1-2% at 1280x720
-  // and 1920x1080 D=256, where a row's stage is 4 columns wide.  The occupancy of each
-  // footprint is looked up once per kernel and size.
+  // three), and only at Dpad 64: measured per shape, the extra rows per SM gain 3% at
+  // 320x240 D=64 (13 rows per SM instead of 10); at Dpad 128 they gained as one launch
+  // set but lose 1.4% on the 848x480 batch once the column kernel leaves room for the
+  // other launch set's rows (seven rows per SM are better there), and at Dpad 256
+  // they lose 1-2%.  The occupancy of each footprint is looked up once per kernel and
+  // size.
   struct Occ { const void* k; size_t sm; int fit; };
   thread_local std::vector<Occ> occ_cache;
   auto fit_of = [&](auto kern, size_t sm) -> int {
@@ -1328,7 +1328,7 @@ cudaError_t launch_rows_t(const DevCfg& cfg, const Batch& b, cudaStream_t s) {
   const int per3 = std::max(1, std::min(fit_of(kern3, sm3), g_rows_ctas_per_sm));
   const int items = b.rows_prefix[b.n];
   cudaError_t e;
-  if (G <= 2 && std::min(items, per2 * nsm) > std::min(items, per3 * nsm)) {
+  if (G == 1 && std::min(items, per2 * nsm) > std::min(items, per3 * nsm)) {
     if ((e = set_smem(kern2, sm2)) != cudaSuccess) return e;
     kern2<<<std::min(items, per2 * nsm), 32 * G, sm2, s>>>(cfg, b);
   } else {
@@ -1402,7 +1402,7 @@ cudaError_t launch_cols_nt(const DevCfg& cfg, const Batch& b0, const de_cfg_hw& 
     }
   }
   if constexpr (KT == 8) {
-    if (pf >= 8 && g_cols_async) {                    // the ring in shared memory
+    if (pf >= 8 && cfg.cols_async) {                  // the ring in shared memory
       constexpr size_t ring_bytes = size_t(NT) * 8 * (KT / 2) * 4;
       const cudaError_t e = set_smem(k_cols<KT, TPCP, 8, NT, true>, ring_bytes);
       if (e != cudaSuccess) return e;

@@ -58,6 +58,7 @@ struct DevCfg {
   int subpixel, fit_eq, lrc;
   float lambda, gamma, damping, keep, min_margin, min_ratio;
   int expire_polls;    // test hook (knob "expire_wait_polls"), 0 = off
+  int cols_async;      // column kernel's prefetch ring in shared memory (knob "cols_async")
   int16_t tbl[66];     // Q14 census score per Hamming distance
   int16_t adt[256];    // Q14 truncated-absolute-difference score
   uint16_t rf[256];    // Q15 filter coefficient per byte difference
@@ -75,10 +76,10 @@ struct Batch {
 };
 
 // de_dense_dev with a bound on the parts a batch runs as on concurrent streams (1: one
-// launch set on `stream`); callers that already overlap batches of their own pass 1
-// (de_capi.cu).
+// launch set on `stream`); callers that already overlap batches of their own pass 1.
+// `reg_ring` keeps the column kernel's prefetch ring in registers (de_capi.cu).
 int dense_dev(const de_cfg* cfg, const de_pair* pairs, int n, void* workspace,
-              size_t ws_bytes, cudaStream_t stream, int max_parts);
+              size_t ws_bytes, cudaStream_t stream, int max_parts, bool reg_ring = false);
 
 // Device address of the no-allocation entry point's status word on the current device
 // (de_noalloc.cu); DE_OK or an error code already recorded for de_last_error().

@@ -181,7 +181,8 @@ DE_API int de_stage_times(float* ms, int n, int* launches);
  *   "cols_async"        1 (default) or 0: at 8 disparities per lane the column
  *                       kernel's 8-row prefetch goes through shared memory by
  *                       asynchronous copies (fewer registers, so more warps and more
- *                       room for a concurrent launch set) instead of a register ring
+ *                       room for a concurrent launch set) instead of a register ring;
+ *                       the host context's chunked batches keep the register ring
  *   "batch_streams"     1..4 (default 2): de_dense_dev runs a batch of several
  *                       pairs as that many parts, pairs taken in turn, each part's
  *                       launch set on its own stream forked from and joined back to

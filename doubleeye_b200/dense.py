@@ -13,6 +13,7 @@ from __future__ import annotations
 import ctypes as C
 import dataclasses
 import threading
+import weakref
 from typing import Optional, Sequence
 
 import numpy as np
@@ -88,10 +89,31 @@ class _Ctx:
 
 
 def _u8(a) -> np.ndarray:
-    a = np.ascontiguousarray(a)
+    if not (isinstance(a, np.ndarray) and a.flags.c_contiguous):
+        a = np.ascontiguousarray(a)
     if a.dtype != np.uint8 or a.ndim != 2:
         raise ValueError("images must be 2-D uint8")
     return a
+
+
+_addr_cache: dict = {}
+
+
+def _addr(a) -> Optional[int]:
+    """Data address of an array.  ``a.ctypes.data`` and ``__array_interface__`` build an
+    object per call; five of them per pair were most of a 16-pair call's host time
+    (about 140 us of a 3.2 ms call), so addresses are cached per array object while it
+    lives, with its size (numpy moves an array's buffer only when its size changes)."""
+    if a is None:
+        return None
+    e = _addr_cache.get(id(a))
+    if e is not None and e[0]() is a and e[1] == a.size:
+        return e[2]
+    p = a.__array_interface__["data"][0]
+    if len(_addr_cache) > 4096:
+        _addr_cache.clear()
+    _addr_cache[id(a)] = (weakref.ref(a), a.size, p)
+    return p
 
 
 def run_dense(left, right, cfg: Optional[DeCfg] = None, *, want_cand: bool = True,
@@ -126,9 +148,9 @@ def run_dense_batch(pairs: Sequence, cfg: Optional[DeCfg] = None, *, want_cand=F
                               np.empty((6, H, W), np.float32) if want_cand else None)
         keep += [L, R]
         outs.append(res)
-        arr[i] = DePair(L.ctypes.data, R.ctypes.data, W, H, int(pr[2]) if len(pr) > 2 else 0,
-                        res.disp.ctypes.data, res.margin.ctypes.data, res.conf.ctypes.data,
-                        res.cand.ctypes.data if want_cand else None)
+        arr[i] = DePair(_addr(L), _addr(R), W, H, int(pr[2]) if len(pr) > 2 else 0,
+                        _addr(res.disp), _addr(res.margin), _addr(res.conf),
+                        _addr(res.cand) if want_cand else None)
     check(lib().de_ctx_dense_batch(ctx, arr, len(pairs)))
     return outs
 

@@ -910,8 +910,11 @@ __device__ __forceinline__ void block_excl_scan(int* a, int n, int* warp_sums) {
   __syncthreads();
 }
 
+// At most 40 registers (six 256-thread CTAs' worth, no spills): the solve still fits
+// five rows per SM by shared memory, and the registers it leaves free let the other
+// launch set's kernels run beside it (the 16-pair batch 2.381 -> 2.376 ms).
 template <bool REF_LAYOUT, int kSolveThreads>
-__global__ void __launch_bounds__(kSolveThreads) k_solve(DevCfg cfg, Batch b) {
+__global__ void __launch_bounds__(kSolveThreads, 1536 / kSolveThreads) k_solve(DevCfg cfg, Batch b) {
   extern __shared__ __align__(128) uint8_t smem[];
   const int item = blockIdx.x;
   const int pi = find_pair(b.solve_prefix, b.n, item);

@@ -102,8 +102,10 @@ _addr_cache: dict = {}
 def _addr(a) -> Optional[int]:
     """Data address of an array.  ``a.ctypes.data`` and ``__array_interface__`` build an
     object per call; five of them per pair were most of a 16-pair call's host time
-    (about 140 us of a 3.2 ms call), so addresses are cached per array object while it
-    lives, with its size (numpy moves an array's buffer only when its size changes)."""
+    (about 100 us of a 3.2 ms call), so addresses are cached per array object while it
+    lives.  The cache holds a weak reference, and numpy refuses to resize in place an
+    array that has one (``ndarray.resize`` raises; ``np.resize`` returns a new array),
+    so a cached address cannot go stale; the size is checked as well."""
     if a is None:
         return None
     e = _addr_cache.get(id(a))
